@@ -1,0 +1,44 @@
+// ============================================================================
+//  launch.h -- host-side launchers exported by the per-precision translation
+//  units (lbm_f64.cu is compiled without FMA contraction so its FP64
+//  arithmetic matches the reference's; lbm_lp.cu holds the FP32/FP16 forms).
+// ============================================================================
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lbm_common.cuh"
+
+namespace lbmgpu {
+
+struct SqArgs;
+
+// launch geometry of one step: the bulk kernel's 3-D grid and the boundary
+// kernel's 1-D grid (0: no boundary nodes)
+struct StreamGeom {
+    dim3 grid, block;
+    unsigned bgrid;
+};
+
+struct Launchers {
+    // one time step of the collide-stream kernels (bulk + boundary)
+    void (*stream)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
+                   cudaStream_t st);
+    // the squirmer update (stages: STAGE_* bits)
+    void (*squirmer)(const Lattice& L, const SqArgs& a, cudaStream_t st);
+    void (*fill_rest)(const Lattice& L, void* f, cudaStream_t st);
+    void (*get_pop)(const Lattice& L, const void* f, const uint8_t* flag, const SqState* sq, int P, int i,
+                    double* out, cudaStream_t st);
+    void (*set_pop)(const Lattice& L, void* f, int P, int i, const double* in, cudaStream_t st);
+    // explicit mass correction: partial sums, final, apply
+    void (*correct_mass)(const Lattice& L, void* f, const uint8_t* flag, int P, SqState* sq, double* part,
+                         double* dflag, cudaStream_t st);
+    cudaError_t (*prepare)();  // one-time function attributes
+};
+
+const Launchers& launchers_f64();
+const Launchers& launchers_f32();
+const Launchers& launchers_f16();
+
+size_t squirmer_smem_bytes();
+
+}  // namespace lbmgpu

@@ -1,0 +1,141 @@
+// ============================================================================
+//  lbm_common.cuh -- lattice constants, node-flag bits, storage forms and the
+//  device-side records shared by the kernels of liblbmgpu.
+// ============================================================================
+#pragma once
+#include <cstdint>
+#include <cuda_fp16.h>
+
+namespace lbmgpu {
+
+// ---- D3Q19, in the reference's order (src/utils/lattice.hpp:18-30) --------
+// Opposite pairs (1,2)(3,4)...(17,18); the order fixes the summation order of
+// the moments, which the FP64 path keeps identical to the reference's.
+constexpr int Q = 19;
+
+__host__ __device__ constexpr int CX(int i) {
+    constexpr int t[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return t[i];
+}
+__host__ __device__ constexpr int CY(int i) {
+    constexpr int t[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+    return t[i];
+}
+__host__ __device__ constexpr int CZ(int i) {
+    constexpr int t[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+    return t[i];
+}
+__host__ __device__ constexpr int OPP(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+__host__ __device__ constexpr double WD(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18 : 1.0 / 36); }
+__host__ __device__ constexpr float WF(int i) { return i == 0 ? 1.0f / 3.0f : (i <= 6 ? 1.0f / 18 : 1.0f / 36); }
+
+// ---- node flag byte ---------------------------------------------------------
+// bits 0-1: node type, same values as the reference's NodeType
+//           (lattice.hpp:36) so the byte's low bits are what the VTK writes;
+// bit 2   : FLUID node with at least one WALL neighbour (static);
+// bit 3   : FLUID node with at least one PARTICLE neighbour (rebuilt with the
+//           boundary-link list whenever the sphere's mapping changes).
+// A FLUID node with bits 2-3 clear streams all 19 populations without a
+// single neighbour-type lookup.
+constexpr uint8_t T_FLUID = 0, T_WALL = 1, T_PARTICLE = 2;
+constexpr uint8_t TYPE_MASK = 3, NEAR_WALL = 4, NEAR_PARTICLE = 8;
+
+// ---- status bits (device error word) --------------------------------------
+constexpr int ST_NAN = 1;            // non-finite force/torque/state
+constexpr int ST_REMAP_RANGE = 2;    // squirmer moved >= 1 cell in one step
+constexpr int ST_LINK_OVERFLOW = 4;  // boundary-link list exceeded its capacity
+constexpr int ST_REMAP_OVERFLOW = 8; // more changed nodes than the remap can order
+
+// ---- storage forms ----------------------------------------------------------
+// FP64: f_i itself. FP32 / FP16: the deviation f_i - w_i rho0 (rho0 = 1), FP16
+// scaled by 2^12 so that typical deviations (1e-8 .. 0.05) stay normal.
+struct StoreF64 {
+    using T = double;
+    static constexpr bool shifted = false;
+    __device__ static double ld(const T* p) { return *p; }
+    __device__ static void st(T* p, double v) { *p = v; }
+    __device__ static double rt(double v) { return v; }  // value as it will be stored
+};
+struct StoreF32 {
+    using T = float;
+    static constexpr bool shifted = true;
+    __device__ static float ld(const T* p) { return *p; }
+    __device__ static void st(T* p, float v) { *p = v; }
+    __device__ static float rt(float v) { return v; }
+};
+constexpr float FP16_SCALE = 4096.0f, FP16_INV_SCALE = 1.0f / 4096.0f;
+struct StoreF16 {
+    using T = __half;
+    static constexpr bool shifted = true;
+    __device__ static float ld(const T* p) { return __half2float(*p) * FP16_INV_SCALE; }
+    __device__ static void st(T* p, float v) { *p = __float2half_rn(v * FP16_SCALE); }
+    __device__ static float rt(float v) { return __half2float(__float2half_rn(v * FP16_SCALE)) * FP16_INV_SCALE; }
+};
+
+// ---- lattice description (kernel argument, fixed per handle) ---------------
+struct Lattice {
+    int nx, ny, nz;
+    unsigned N;            // nx*ny*nz (< 2^31)
+    unsigned nxy;
+    int walls_y, walls_z;
+    double omP, omM, gP, gM, F[3];  // TRT rates and Guo factors (lbm.cpp:65-69, :129)
+    // FP32 copies and per-direction forcing constants of the shifted forms:
+    // cF[i] = c_i . F and cm[i] = gM * 3 w_i (c_i . F) for the odd i of each pair
+    float omPf, omMf, gPf, gMf, Ff[3], uFh[3];
+    float cF[Q], cm[Q];
+};
+
+// ---- squirmer / run state on the device ------------------------------------
+// Everything the per-step kernels need to decide and compute without a host
+// round trip. FP64 throughout.
+struct SqState {
+    // model (squirmer.hpp:16-18, :35-36)
+    double R, B1, beta, M, I, eps, hc, hmin, FS;
+    int planar, present;
+    // rigid-body state (squirmer.hpp:22-31)
+    double X[3], e[3], U[3], W[3];
+    double Fh[3], Th[3], Fc[3], Tc[3], Fw[3];
+    long long contacts;
+    // step bookkeeping
+    long long t;                 // completed squirmer updates (= time steps in run mode)
+    long long n_fluid;           // number of FLUID nodes
+    int mass_every, traj_every;
+    int corr_pending;            // apply f_i += w_i * corr_d on the next load
+    double corr_d;
+    // region of nodes whose rho the next step must store (for the refill)
+    int rb_lo[3], rb_w[3];       // wrapped lower corner, width (<= extent)
+    int rb_valid;
+    // boundary-link list
+    int n_links;
+    // last wall force (written on macro steps)
+    double wall_force[3];
+    // trajectory ring
+    long long traj_count;
+    int status;
+};
+
+constexpr int TRAJ_RING = 4096;
+constexpr int TRAJ_COLS = 15;
+
+// Per-node partial sums written by the stream kernel for boundary-link nodes:
+// F (3), T (3), and two spare slots.
+constexpr int LINK_PART = 8;
+// Per-block partials of the stream kernel on reduction steps: wall force (3), mass (1).
+constexpr int BLOCK_PART = 4;
+
+struct StreamArgs {
+    void* f;                      // populations, SoA f[i*N + n]
+    uint8_t* flag;
+    double* rho;                  // pre-collision moments (FP64)
+    double* ux; double* uy; double* uz;
+    double* link_part;            // [n_links][LINK_PART], one row per near-particle node
+    double* block_part;           // bulk kernel: [blocks][BLOCK_PART]
+    double* block_part_b;         // boundary kernel: [blocks][BLOCK_PART]
+    const int* wall_nodes;        // static list: non-wall nodes with a WALL neighbour
+    int n_wall;
+    const int* links;             // boundary-link list (near-particle nodes)
+    SqState* sq;
+    int fused;                    // 1: time-loop mode (mass sums on correction steps)
+};
+
+}  // namespace lbmgpu

@@ -1,0 +1,84 @@
+// ============================================================================
+//  lbm_launch_impl.cuh -- launcher table for one storage form (included by
+//  exactly one translation unit per form).
+// ============================================================================
+#pragma once
+#include "k_aux.cuh"
+#include "k_squirmer.cuh"
+#include "k_stream.cuh"
+#include "launch.h"
+
+namespace lbmgpu {
+
+template <class S, int PAR, bool SQ, bool MACRO>
+static void stream_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    k_bulk<S, PAR, SQ, MACRO><<<g.grid, g.block, 0, st>>>(L, a);
+    if (g.bgrid) k_boundary<S, PAR, SQ, MACRO><<<g.bgrid, BOUNDARY_BLOCK, 0, st>>>(L, a);
+}
+
+template <class S>
+static void stream_dispatch(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& grid,
+                            cudaStream_t st) {
+    const int key = (par ? 4 : 0) | (sq ? 2 : 0) | (macro ? 1 : 0);
+    switch (key) {
+        case 0: stream_one<S, 0, false, false>(L, a, grid, st); break;
+        case 1: stream_one<S, 0, false, true>(L, a, grid, st); break;
+        case 2: stream_one<S, 0, true, false>(L, a, grid, st); break;
+        case 3: stream_one<S, 0, true, true>(L, a, grid, st); break;
+        case 4: stream_one<S, 1, false, false>(L, a, grid, st); break;
+        case 5: stream_one<S, 1, false, true>(L, a, grid, st); break;
+        case 6: stream_one<S, 1, true, false>(L, a, grid, st); break;
+        default: stream_one<S, 1, true, true>(L, a, grid, st); break;
+    }
+}
+
+inline size_t squirmer_smem() { return sizeof(ChgSh) * SQ_BATCH; }
+
+template <class S>
+static void squirmer_launch(const Lattice& L, const SqArgs& a, cudaStream_t st) {
+    k_squirmer<S><<<1, SQ_THREADS, squirmer_smem(), st>>>(L, a);
+}
+
+template <class S>
+static void fill_launch(const Lattice& L, void* f, cudaStream_t st) {
+    k_fill_rest<S><<<1184, AUX_BLOCK, 0, st>>>(L, f);
+}
+
+template <class S>
+static void get_pop_launch(const Lattice& L, const void* f, const uint8_t* flag, const SqState* sq, int P, int i,
+                           double* out, cudaStream_t st) {
+    k_get_pop<S><<<1184, AUX_BLOCK, 0, st>>>(L, f, flag, sq, P, i, out);
+}
+
+template <class S>
+static void set_pop_launch(const Lattice& L, void* f, int P, int i, const double* in, cudaStream_t st) {
+    k_set_pop<S><<<1184, AUX_BLOCK, 0, st>>>(L, f, P, i, in);
+}
+
+template <class S>
+static void correct_mass_launch(const Lattice& L, void* f, const uint8_t* flag, int P, SqState* sq, double* part,
+                                double* dflag, cudaStream_t st) {
+    k_mass_partial<S><<<MASS_GRID, AUX_BLOCK, 0, st>>>(L, f, flag, P, part);
+    k_mass_final<S><<<1, 32, 0, st>>>(part, MASS_GRID, sq, dflag);
+    k_mass_apply<S><<<1184, AUX_BLOCK, 0, st>>>(L, f, flag, P, sq, dflag);
+}
+
+template <class S>
+static cudaError_t prepare_launch() {
+    return cudaFuncSetAttribute(k_squirmer<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+}
+
+template <class S>
+static Launchers make_launchers() {
+    Launchers l;
+    l.stream = &stream_dispatch<S>;
+    l.squirmer = &squirmer_launch<S>;
+    l.fill_rest = &fill_launch<S>;
+    l.get_pop = &get_pop_launch<S>;
+    l.set_pop = &set_pop_launch<S>;
+    l.correct_mass = &correct_mass_launch<S>;
+    l.prepare = &prepare_launch<S>;
+    return l;
+}
+
+}  // namespace lbmgpu

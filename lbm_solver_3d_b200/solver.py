@@ -1,0 +1,126 @@
+"""Python face of the CUDA library: the reference's ``lbm::LBM`` interface.
+
+``Solver(params)`` mirrors ``LBM::LBM(const Params&)`` (src/utils/lbm.cpp:60-94)
+and exposes ``step()``, ``advance_squirmer()``, ``correct_mass()`` (lbm.cpp:128,
+:257, :324), the diagnostics (lbm.cpp:342-364) and the fields the output
+writers read, plus ``run(n)``: n iterations of the time-loop body of
+src/main.cpp:60-64 executed on the device in CUDA graphs. Every call goes
+through the C ABI of include/lbmgpu.h; there is no CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import LbmgpuDiagnostics, LbmgpuSquirmer, check, dptr, u8ptr
+from .params import Params
+
+Q = 19
+
+
+class Solver:
+    def __init__(self, params: Params):
+        params.validate()
+        self.params = params
+        self.lib = _lib.load()
+        self.N = params.ncells
+        self.shape = (params.NZ, params.NY, params.NX)
+        c = params.to_c()
+        h = ctypes.c_void_p()
+        check(self.lib.lbmgpu_create(ctypes.byref(c), ctypes.byref(h)), None)
+        self.h = h
+
+    # ---- the reference's three per-step calls ----
+    def step(self) -> None:
+        check(self.lib.lbmgpu_step(self.h), self.h)
+
+    def advance_squirmer(self) -> None:
+        check(self.lib.lbmgpu_advance_squirmer(self.h), self.h)
+
+    def correct_mass(self) -> None:
+        check(self.lib.lbmgpu_correct_mass(self.h), self.h)
+
+    # ---- the fused time loop ----
+    def run(self, nsteps: int) -> None:
+        check(self.lib.lbmgpu_run(self.h, int(nsteps)), self.h)
+
+    @property
+    def t(self) -> int:
+        v = ctypes.c_longlong()
+        check(self.lib.lbmgpu_time(self.h, ctypes.byref(v)), self.h)
+        return v.value
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        check(self.lib.lbmgpu_launch_count(self.h, ctypes.byref(v)), self.h)
+        return v.value
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        check(self.lib.lbmgpu_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), self.h)
+
+    # ---- state ----
+    def squirmer(self) -> dict:
+        s = LbmgpuSquirmer()
+        check(self.lib.lbmgpu_squirmer_state(self.h, ctypes.byref(s)), self.h)
+        out = {k: np.array(getattr(s, k)[:]) for k in ("X", "e", "U", "W", "Fh", "Th", "Fc", "Tc", "Fw")}
+        out.update(R=s.R, B1=s.B1, beta=s.beta, M=s.M, I=s.I, FS=s.FS, U0=s.U0, contacts=int(s.contacts))
+        return out
+
+    def set_squirmer(self, X, e, U, W) -> None:
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (X, e, U, W)]
+        check(self.lib.lbmgpu_set_squirmer_state(self.h, *[dptr(v) for v in a]), self.h)
+
+    def fields(self):
+        """(flag, rho, u) as arrays indexed [z, y, x] and [z, y, x, 3]."""
+        flag = np.empty(self.N, np.uint8)
+        rho = np.empty(self.N)
+        u = np.empty(3 * self.N)
+        check(self.lib.lbmgpu_fields(self.h, u8ptr(flag), dptr(rho), dptr(u)), self.h)
+        return flag.reshape(self.shape), rho.reshape(self.shape), u.reshape(self.shape + (3,))
+
+    def diag(self) -> dict:
+        d = LbmgpuDiagnostics()
+        check(self.lib.lbmgpu_diag(self.h, ctypes.byref(d)), self.h)
+        return dict(n_fluid=int(d.n_fluid), mean_density=d.mean_density, max_speed=d.max_speed,
+                    sum_ux=d.sum_ux, wall_force=np.array(d.wall_force[:]))
+
+    def wall_force(self) -> np.ndarray:
+        return self.diag()["wall_force"]
+
+    def traj_rows(self, max_rows: int = 1 << 16) -> np.ndarray:
+        buf = np.empty((max_rows, 15))
+        n = ctypes.c_int()
+        dropped = ctypes.c_longlong()
+        check(self.lib.lbmgpu_traj_rows(self.h, dptr(buf), max_rows, ctypes.byref(n), ctypes.byref(dropped)), self.h)
+        if dropped.value:
+            raise RuntimeError(f"{dropped.value} trajectory rows were overwritten before being read")
+        return buf[: n.value].copy()
+
+    def get_f(self) -> np.ndarray:
+        f = np.empty(Q * self.N)
+        check(self.lib.lbmgpu_get_populations(self.h, dptr(f)), self.h)
+        return f.reshape((Q,) + self.shape)
+
+    def set_f(self, f) -> None:
+        f = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
+        assert f.size == Q * self.N
+        check(self.lib.lbmgpu_set_populations(self.h, dptr(f)), self.h)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.lbmgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,84 @@
+"""The C ABI library loads, exports every symbol include/lbmgpu.h declares, and
+its host-side entry points behave like the reference's Params (no GPU needed:
+nothing here launches a kernel)."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from lbm_solver_3d_b200 import _lib
+from lbm_solver_3d_b200.params import ParamError, Params
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    text = (ROOT / "include" / "lbmgpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lbmgpu_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in include/lbmgpu.h but not exported"
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+    assert lib.lbmgpu_abi_version() == 1
+
+
+def test_defaults_are_the_reference_defaults():
+    lib = _lib.load()
+    c = _lib.LbmgpuParams()
+    lib.lbmgpu_params_default(ctypes.byref(c))
+    ref = Params().to_c()
+    for name, _ in _lib.LbmgpuParams._fields_:
+        assert getattr(c, name) == getattr(ref, name), name
+
+
+INVALID = [
+    (dict(nx=0), "grid dimensions must be positive"),
+    (dict(ny=3, walls_y=1), "ny must be >= 4 with walls in y"),
+    (dict(nz=3, walls_z=1), "nz must be >= 4 with walls in z"),
+    (dict(tau=0.5), "tau must be > 0.5"),
+    (dict(**{"lambda": 0}), "lambda must be > 0"),
+    (dict(traj_every=0), "print_every and traj_every must be >= 1"),
+    (dict(squirmer=1, radius=1.0), "squirmer radius must be > 1 lattice unit"),
+    (dict(squirmer=1, angle=45), "initial angle must satisfy |angle| < 45 deg from the x-axis"),
+    (dict(squirmer=1, rho_p=0), "rho_p must be > 0"),
+    (dict(squirmer=1, hc=0), "eps >= 0, hc > 0, hmin >= 0 required"),
+    (dict(squirmer=1, y0=4.0), "squirmer initially overlaps (or is too close to) a y-wall"),
+    (dict(squirmer=1, nx=9), "domain too small for the squirmer"),
+    (dict(squirmer=1, b1=0.08), "swimming speed U0 = 2 B1 / 3 too large (Mach number); keep U0 < 0.05"),
+]
+
+
+@pytest.mark.parametrize("kw,msg", INVALID)
+def test_validate_messages_match_reference_rules(kw, msg):
+    """lbmgpu_validate (C) and Params.validate (Python) both apply
+    params.cpp:120-140 with its messages."""
+    p = Params().update(**kw)
+    with pytest.raises(ParamError, match=re.escape(msg)):
+        p.validate()
+    lib = _lib.load()
+    buf = ctypes.create_string_buffer(256)
+    rc = lib.lbmgpu_validate(ctypes.byref(p.to_c()), buf, 256)
+    assert rc == -1 and buf.value.decode() == msg
+
+
+def test_create_fails_loudly_without_a_device_or_with_bad_params():
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    bad = Params().update(tau=0.4).to_c()
+    assert lib.lbmgpu_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    assert b"tau must be > 0.5" in lib.lbmgpu_last_error(None)
+    assert not h.value
+
+
+def test_null_handles_are_rejected():
+    lib = _lib.load()
+    assert lib.lbmgpu_run(None, 1) == -1
+    assert lib.lbmgpu_step(None) == -1
+    assert lib.lbmgpu_destroy(None) == 0

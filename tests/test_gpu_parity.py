@@ -1,0 +1,225 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+The oracle is the plain-C restatement (oracle/lbm_oracle.c), itself pinned bit
+for bit to the reference compiled from its own sources (tests/test_oracle.py).
+
+Tolerances
+  * one step, FP64: bit-identical populations and moments (the FP64 kernels
+    use the reference's operation order without FMA contraction); forces
+    differ only by summation order (relative 1e-12);
+  * multi-step FP64: relative L2 <= 1e-10 in rho, u, populations and the
+    squirmer position/orientation (the target for the plain method);
+  * FP32-shifted: relative L2 of u <= 1e-5 against the FP64 oracle;
+  * FP16 storage: error reported, bound 5e-2 (a sanity bound, not a target).
+"""
+import numpy as np
+import pytest
+
+from lbm_solver_3d_b200.params import Params
+
+pytestmark = pytest.mark.gpu
+
+Q = 19
+W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, float).ravel()
+    b = np.asarray(b, float).ravel()
+    den = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (den if den > 0 else 1.0)
+
+
+CASES = {
+    # duct with a 3-component body force, walls in y and z
+    "duct": dict(nx=12, ny=14, nz=10, tau=0.8, fx=1e-5, fy=2e-6, fz=-3e-6, walls_y=1, walls_z=1, squirmer=0),
+    # slit channel with a squirmer (the reference's channel deck, smaller)
+    "slit": dict(nx=40, ny=26, nz=22, tau=1.0, walls_y=1, walls_z=0, squirmer=1, radius=4.5, b1=0.015,
+                 beta=-2.0, angle=20, planar=1),
+    # fully periodic box, 3-D orientation, non-planar
+    "bulk3d": dict(nx=24, ny=22, nz=20, tau=0.9, walls_y=0, walls_z=0, squirmer=1, radius=4.2, b1=0.01,
+                   beta=3.0, planar=0, ex=0.3, ey=-0.5, ez=0.8),
+    # duct walls and a squirmer near a z wall
+    "boxwalls": dict(nx=30, ny=24, nz=24, tau=0.75, walls_y=1, walls_z=1, squirmer=1, radius=5.0, b1=0.012,
+                     beta=1.0, angle=-10, planar=0, z0=8.0, y0=13.0),
+}
+
+
+def make_params(name, **kw):
+    p = Params()
+    p.update(**CASES[name])
+    p.update(**kw)
+    p.validate()
+    return p
+
+
+def seeded_state(p, seed):
+    """Perturbed populations (all 19 directions non-trivial) and a moving sphere."""
+    rng = np.random.default_rng(seed)
+    f = W[:, None, None, None] * (1.0 + 0.02 * rng.standard_normal((Q, p.NZ, p.NY, p.NX)))
+    return f
+
+
+@pytest.fixture(scope="module")
+def port(oracle_mod):
+    oracle_mod.set_threads(8)
+    return oracle_mod.PortSolver
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from lbm_solver_3d_b200.solver import Solver
+    return Solver
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(CASES))
+def test_single_step_bitwise_fp64(case, port, Solver):
+    p = make_params(case)
+    g, o = Solver(p), port(p)
+    f0 = seeded_state(p, 11)
+    g.set_f(f0); o.set_f(f0)
+    if p.squirmer:
+        st = o.squirmer()
+        U = np.array([0.004, -0.003, 0.002 if not p.planar else 0.0])
+        Wv = np.array([0.0, 0.0, 0.001]) if p.planar else np.array([0.0005, -0.0007, 0.001])
+        g.set_squirmer(st["X"], st["e"], U, Wv)
+        o.set_squirmer(st["X"], st["e"], U, Wv)
+    for k in range(2):  # an even and an odd AA step
+        g.step(); o.step()
+        fg, fo = g.get_f(), o.get_f()
+        fl, rg, ug = g.fields()
+        _, ro, uo = o.fields()
+        fluid = fl == 0
+        assert np.array_equal(fg[:, fluid], fo[:, fluid]), f"step {k}: populations differ (max {np.abs(fg - fo).max():.3e})"
+        assert np.array_equal(rg[fluid], ro[fluid]) and np.array_equal(ug[fluid], uo[fluid])
+        # sums of O(1e3) link terms in another order: rounding only
+        wg, wo = g.wall_force(), o.wall_force()
+        assert np.allclose(wg, wo, rtol=1e-10, atol=1e-13)
+        if p.squirmer:
+            sg, so = g.squirmer(), o.squirmer()
+            assert np.allclose(sg["Fh"], so["Fh"], rtol=1e-10, atol=1e-13)
+            assert np.allclose(sg["Th"], so["Th"], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("case", ["slit", "bulk3d", "boxwalls"])
+def test_advance_squirmer_remap_fp64(case, port, Solver):
+    """Rigid-body update and cover/uncover remap (lbm.cpp:257-320), forced to
+    move the sphere by 0.45 cells so that dozens of nodes change type."""
+    p = make_params(case)
+    g, o = Solver(p), port(p)
+    f0 = seeded_state(p, 5)
+    g.set_f(f0); o.set_f(f0)
+    st = o.squirmer()
+    U = np.array([0.45, -0.3, 0.0 if p.planar else 0.2])
+    Wv = np.array([0.0, 0.0, 0.02]) if p.planar else np.array([0.01, -0.02, 0.02])
+    g.set_squirmer(st["X"], st["e"], U, Wv)
+    o.set_squirmer(st["X"], st["e"], U, Wv)
+    for _ in range(2):
+        flag_before = o.fields()[0].copy()
+        g.step(); o.step()
+        g.advance_squirmer(); o.advance_squirmer()
+        sg, so = g.squirmer(), o.squirmer()
+        for k in ("X", "e", "U", "W", "Fc", "Tc", "Fw"):
+            assert np.allclose(sg[k], so[k], rtol=1e-11, atol=1e-14), (k, sg[k], so[k])
+        assert sg["contacts"] == so["contacts"]
+        flg, rg, ug = g.fields()
+        flo, ro, uo = o.fields()
+        assert np.array_equal(flg, flo)
+        changed = flag_before != flo
+        assert changed.sum() > 10
+        fluid = flo == 0
+        fg, fo = g.get_f(), o.get_f()
+        assert rel_l2(fg[:, fluid], fo[:, fluid]) < 1e-14
+        unc = changed & fluid
+        assert np.allclose(rg[unc], ro[unc], rtol=1e-13) and np.allclose(ug[unc], uo[unc], rtol=1e-12, atol=1e-16)
+
+
+@pytest.mark.parametrize("case", ["duct", "slit"])
+def test_correct_mass_fp64(case, port, Solver):
+    p = make_params(case)
+    g, o = Solver(p), port(p)
+    f0 = seeded_state(p, 3)
+    g.set_f(f0); o.set_f(f0)
+    g.step(); o.step()
+    g.correct_mass(); o.correct_mass()
+    fl = o.fields()[0]
+    fluid = fl == 0
+    fg, fo = g.get_f()[:, fluid], o.get_f()[:, fluid]
+    assert rel_l2(fg, fo) < 1e-14   # d from sums in another order
+    m = fg.sum() / fluid.sum()
+    assert abs(m - 1.0) < 1e-13
+
+
+@pytest.mark.parametrize("case,steps", [("duct", 1500), ("slit", 600), ("bulk3d", 400), ("boxwalls", 400)])
+def test_run_matches_oracle_fp64(case, steps, port, Solver):
+    """The fused device loop (CUDA graphs, deferred mass correction, device
+    trajectory ring) against the oracle's time loop."""
+    p = make_params(case, traj_every=10, mass_correction_every=10)
+    g, o = Solver(p), port(p)
+    g.run(steps)
+    to = o.run(steps)
+    fl, rg, ug = g.fields()
+    flo, ro, uo = o.fields()
+    assert np.array_equal(fl, flo)
+    fluid = flo == 0
+    assert rel_l2(rg[fluid], ro[fluid]) < 1e-10
+    assert rel_l2(ug[fluid], uo[fluid]) < 1e-10
+    assert rel_l2(g.get_f()[:, fluid], o.get_f()[:, fluid]) < 1e-10
+    dg, do = g.diag(), o.diag()
+    assert dg["n_fluid"] == do["n_fluid"]
+    assert abs(dg["mean_density"] - do["mean_density"]) < 1e-12
+    assert abs(dg["max_speed"] - do["max_speed"]) <= 1e-10 * do["max_speed"]
+    assert np.allclose(dg["wall_force"], o.wall_force(), rtol=1e-9, atol=1e-14)
+    if p.squirmer:
+        tg = g.traj_rows()
+        assert tg.shape == to.shape
+        assert np.array_equal(tg[:, 0], to[:, 0])
+        assert rel_l2(tg[:, 1:4], to[:, 1:4]) < 1e-10  # X
+        assert rel_l2(tg[:, 4:7], to[:, 4:7]) < 1e-10  # e
+        assert rel_l2(tg[:, 7:10], to[:, 7:10]) < 1e-8  # U
+        sg, so = g.squirmer(), o.squirmer()
+        assert sg["contacts"] == so["contacts"]
+
+
+def test_run_equals_granular_calls(Solver):
+    """run(n) (graphs, deferred correction) equals n explicit
+    step/advance_squirmer/correct_mass calls, up to summation-order rounding."""
+    p = make_params("slit", mass_correction_every=10)
+    a, b = Solver(p), Solver(p)
+    a.run(137)
+    for t in range(1, 138):
+        b.step(); b.advance_squirmer()
+        if t % 10 == 0:
+            b.correct_mass()
+    sa, sb = a.squirmer(), b.squirmer()
+    for k in ("X", "e", "U", "W"):
+        assert np.allclose(sa[k], sb[k], rtol=1e-12, atol=1e-16), k
+    fluid = a.fields()[0] == 0
+    assert rel_l2(a.get_f()[:, fluid], b.get_f()[:, fluid]) < 1e-13
+
+
+def test_deterministic(Solver):
+    p = make_params("bulk3d")
+    a, b = Solver(p), Solver(p)
+    a.run(200); b.run(200)
+    assert np.array_equal(a.get_f(), b.get_f())
+    assert np.array_equal(a.squirmer()["X"], b.squirmer()["X"])
+
+
+@pytest.mark.parametrize("prec,bound", [("fp32", 1e-5), ("fp16", 5e-2)])
+def test_precision_forms_error(prec, bound, port, Solver):
+    p64 = make_params("slit")
+    o = port(p64)
+    o.run(400)
+    g = Solver(make_params("slit", precision=prec))
+    g.run(400)
+    fl, rg, ug = g.fields()
+    flo, ro, uo = o.fields()
+    fluid = (fl == 0) & (flo == 0)
+    err_u = rel_l2(ug[fluid], uo[fluid])
+    err_rho = rel_l2(rg[fluid] - 1.0, ro[fluid] - 1.0)
+    sg, so = g.squirmer(), o.squirmer()
+    drift = np.linalg.norm(sg["X"] - so["X"]) / np.linalg.norm(so["X"] - np.array([19.5, 12.5, 10.5]))
+    print(f"{prec}: rel L2 u {err_u:.3e}, rho-1 {err_rho:.3e}, drift {drift:.3e}")
+    assert err_u < bound
