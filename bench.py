@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""Throughput of the D3Q19 TRT + squirmer time step on B200, as MLUPS.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32]
+                    [--workload bulk_0] [--impl ours|reference]
+
+Workload (default): the precision/roofline sweep lattice -- a fully periodic
+256x128x128 box with one squirmer (a=8, beta=0, B1=1e-3, tau=0.9, seeded 3-D
+orientation), FP32-shifted populations. A "step" is one time step of the whole
+hot path (collide-stream + bounce-back + momentum exchange + rigid body +
+remap + mass correction every 10 steps), run through the C ABI's time loop.
+The populations (319 MB in FP32) are larger than the 126 MB L2, so no flush is
+needed between steps. MLUPS counts every lattice node, as the reference does
+(src/main.cpp:90).
+
+One process per GPU (torchrun for N > 1): each rank advances its own replica of
+the lattice -- a single lattice is not split across GPUs -- so scaling is weak
+and `value` is the sum over ranks (cells x steps / slowest rank's time).
+
+--impl reference times the reference's own CPU code (compiled from its sources
+into oracle/_ref) on the host cores, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS & %HBM roofline FP64 vs FP32-shifted at ≤1e-5 err; sweep trajectories/hr"
+BYTES = {"fp64": 8, "fp32": 4, "fp16": 2}
+DTYPE = {"fp64": "f64", "fp32": "f32-shifted", "fp16": "f16-storage/f32-math"}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(p, seconds_target=15.0):
+    """The reference's own code (oracle/_ref, compiled from its sources) on the
+    host cores: a bounded sample of the same workload."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    if not oracle.ref_available():
+        s = oracle.PortSolver(p)
+        kind = "port"
+    else:
+        s = oracle.RefSolver(p)
+        kind = "reference"
+    s.run(1)  # first touch
+    steps, t = 1, 0.0
+    while True:
+        t0 = time.perf_counter()
+        s.run(steps)
+        t = time.perf_counter() - t0
+        if t > 0.25 * seconds_target or steps >= 256:
+            break
+        steps *= 2
+    mlups = p.ncells * steps / t / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
+            "sample": f"{p.NX}x{p.NY}x{p.NZ} lattice, {steps} time steps after 1 warm-up step, "
+                      f"{threads} OpenMP threads, FP64 (the reference's only form)"}
+
+
+def run_reference_arm(args, p):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    kind = "reference" if oracle.ref_available() else "port"
+    s = oracle.RefSolver(p) if kind == "reference" else oracle.PortSolver(p)
+    for _ in range(args.warmup):
+        s.run(1)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s.run(1)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    mlups = p.ncells * args.steps / tot / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args, p, reference=True),
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} time steps of the workload after {args.warmup} warm-up steps, "
+                                   f"{threads} OpenMP threads"},
+        "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, p, reference=False):
+    return {"workload": f"{args.workload}: periodic {p.NX}x{p.NY}x{p.NZ} box, one squirmer "
+                        f"a={p.R:g} beta={p.beta:g} B1={p.B1:g} tau={p.tau:g}, seeded 3-D orientation"
+            if p.squirmer else f"{args.workload}: {p.NX}x{p.NY}x{p.NZ}",
+            "cells": p.ncells, "precision": "fp64" if reference else args.precision,
+            "mass_correction_every": p.massCorrectionEvery,
+            "l2": "populations larger than L2 (126 MB); no flush",
+            "parallelism": f"replica per GPU x{dist_env()[0]}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--precision", default="fp32", choices=list(BYTES))
+    ap.add_argument("--workload", default="bulk_0")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    from lbm_solver_3d_b200.workloads import workload_params
+    p = workload_params(args.workload, "fp64" if args.impl == "reference" else args.precision)
+
+    if args.impl == "reference":
+        run_reference_arm(args, p)
+        return
+
+    world, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    p.update(device=local)
+    from lbm_solver_3d_b200.solver import Solver
+
+    stream = torch.cuda.Stream(device=local)
+    sol = Solver(p)
+    sol.set_stream(stream.cuda_stream)
+    sol.run(args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K time steps on the device, inputs resident in HBM ----
+    l0 = sol.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            sol.run(args.steps)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = sol.launch_count() - l0
+    t_max = torch.tensor([ms], device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t_max, op=pg.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * p.ncells * args.steps / (ms_max * 1e-3) / 1e6
+
+    # ---- dominant kernel alone (CUDA events on the library's stream) ----
+    kt = sol.time_kernels(reps=20)
+    sol.close()
+    peak, peak_kind = peaks()
+    bytes_per_launch = 2 * 19 * BYTES[args.precision] * p.ncells
+    achieved = bytes_per_launch / (kt["bulk"] * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(f"k_bulk:{args.workload}:{args.precision}")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the C ABI: create from host params, run, read results ----
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = Solver(p)
+    traj_bytes = 0
+    remaining = args.steps
+    chunk = max(p.trajEvery, min(remaining, 1000))
+    while remaining > 0:
+        k = min(chunk, remaining)
+        s2.run(k)
+        traj_bytes += s2.traj_rows().nbytes
+        remaining -= k
+    flag, rho, u = s2.fields()
+    t_e2e = time.perf_counter() - t0
+    s2.close()
+    h2d = p.ncells * 1 + 4 * (p.ncells if p.squirmer else 0)  # flags + boundary-link set-up
+    d2h = traj_bytes + flag.nbytes + rho.nbytes + u.nbytes
+    e2e_val = p.ncells * args.steps / t_e2e / 1e6
+    e2e = {"value": world * e2e_val, "unit": "MLUPS",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "what": "lbmgpu_create (host set-up and upload) + lbmgpu_run in chunks + trajectory rows "
+                   "+ final flag/rho/u fields to host, wall clock per rank"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
+            "config": workload_config(args, p),
+            "roofline": {"bound": "hbm", "kernel": "k_bulk (collide-stream, AA, bulk nodes)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "bytes_per_launch": bytes_per_launch, "launch_ms": kt["bulk"],
+                         "per_unit": f"2 x 19 x {BYTES[args.precision]} B per lattice node"},
+            "step_breakdown_ms": kt,
+            "step_roofline_frac": (bytes_per_launch / (ms_max / args.steps * 1e-3) / 1e9) / peak,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "e2e": e2e,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            q = workload_params(args.workload, "fp64")
+            line["cpu_baseline"] = cpu_baseline(q)
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

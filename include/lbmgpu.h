@@ -165,6 +165,16 @@ int lbmgpu_set_stream(lbmgpu_handle* h, void* cuda_stream);
  * every kernel node they run). */
 int lbmgpu_launch_count(const lbmgpu_handle* h, long long* n);
 
+/* Measurement aid (no counterpart in the reference): times the kernels of one
+ * time step separately with CUDA events on the handle's stream, `reps`
+ * launches each (reps is rounded up to an even number so the AA parity is
+ * preserved). ms[0] = bulk collide-stream kernel, ms[1] = boundary/zone
+ * kernel (0 if there is none), ms[2] = squirmer kernel (0 without a squirmer);
+ * averages per launch. The populations advance `reps` steps without the
+ * sphere update in between, so the physical state is no longer meaningful
+ * afterwards: use it on a handle kept for measurement. */
+int lbmgpu_time_kernels(lbmgpu_handle* h, int reps, double ms[3]);
+
 /* Message of the last failure on this handle (or of lbmgpu_create on the
  * calling thread when h is NULL). Never NULL. */
 const char* lbmgpu_last_error(const lbmgpu_handle* h);

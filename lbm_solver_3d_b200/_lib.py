@@ -74,6 +74,7 @@ SIGNATURES = {
     "lbmgpu_set_squirmer_state": (_I, [_P, _DP, _DP, _DP, _DP]),
     "lbmgpu_set_stream": (_I, [_P, _P]),
     "lbmgpu_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "lbmgpu_time_kernels": (_I, [_P, _I, _DP]),
     "lbmgpu_last_error": (ctypes.c_char_p, [_P]),
     "lbmgpu_abi_version": (_I, []),
 }

@@ -44,12 +44,15 @@ struct SqArgs {
     uint8_t* flag;
     double* rho; double* ux; double* uy; double* uz;
     int* links;
+    int* linkslot;            // node -> row of its boundary-link entry
     int link_cap;
     const double* link_part;
     const double* block_part;     // bulk kernel partials (mass in column 3)
     int nblocks;
-    const double* block_part_b;   // boundary kernel partials
+    const double* block_part_b;   // zone kernel partials
     int nblocks_b;
+    const double* block_part_w;   // wall-row partials of an ensemble member (else unused)
+    int nblocks_w;
     int* ordermap;            // N entries, -1 when idle
     int* chg_node;            // changed-node list (capacity chg_cap)
     int* chg_key;
@@ -60,6 +63,8 @@ struct SqArgs {
     SqState* sq;
     int parity;               // parity of the state being remapped
     int stages;
+    int corr_step;            // this step is a mass-correction step (time-loop mode)
+    int zslot_a, zslot_b;     // zone slots to (re)write from the new position, -1: none
 };
 
 struct ChgSh {
@@ -123,7 +128,7 @@ struct AxisRange {
 };
 
 template <class S>
-__global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const SqArgs a) {
+__device__ void squirmer_update(const Lattice& L, const SqArgs& a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ChgSh* ch = reinterpret_cast<ChgSh*>(smem_raw);
     __shared__ SqState s;
@@ -146,7 +151,7 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
 
     const long long t_now = s.t + 1;
     const bool loop = (a.stages & STAGE_LOOP) != 0;
-    const bool corr_step = loop && s.mass_every > 0 && (t_now % s.mass_every) == 0;
+    const bool corr_step = loop && a.corr_step;
 
     // ---------------- stage BODY ----------------
     if (a.stages & STAGE_FORCE) {
@@ -514,6 +519,7 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
                     const int n = a.cand[c];
                     if (off < a.link_cap) {
                         a.links[off] = n;
+                        a.linkslot[n] = off;
                         a.flag[n] |= NEAR_PARTICLE;
                     }
                     ++off;
@@ -535,6 +541,10 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
         mstep = sums[0];
         block_sum_rows<1>(a.block_part_b, a.nblocks_b, BLOCK_PART, 3, sums);
         mstep += sums[0];
+        if (a.nblocks_w > 0) {
+            block_sum_rows<1>(a.block_part_w, a.nblocks_w, BLOCK_PART, 3, sums);
+            mstep += sums[0];
+        }
     }
     if (tid == 0) {
         if (loop) {
@@ -558,17 +568,43 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
         } else {
             s.corr_pending = 0;
         }
-        // densities the next step stores: this box widened by 2
-        const int lo[3] = {bx0 - 2, by0 - 2, bz0 - 2};
-        const int w[3] = {bw + 4, bh + 4, bd + 4};
+        // zones of the coming steps, from this box (see ZoneBox)
+        const int blo[3] = {bx0, by0, bz0};
         const int nd[3] = {L.nx, L.ny, L.nz};
-        for (int d = 0; d < 3; ++d) {
-            s.rb_w[d] = min(w[d], nd[d]);
-            s.rb_lo[d] = w[d] >= nd[d] ? 0 : ((lo[d] % nd[d]) + nd[d]) % nd[d];
+        const bool wall_axis[3] = {false, L.walls_y != 0, L.walls_z != 0};
+        for (int slot : {a.zslot_a, a.zslot_b}) {
+            if (slot < 0) continue;
+            for (int d = 0; d < 3; ++d) {
+                s.zone[slot].w[d] = zone_width(s.R, nd[d], wall_axis[d]);
+                zone_axis(blo[d], nd[d], s.zone[slot].w[d], wall_axis[d], s.zone[slot].lo[d]);
+            }
         }
-        s.rb_valid = 1;
         *a.sq = s;
     }
+}
+
+template <class S>
+__global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const SqArgs a) {
+    squirmer_update<S>(L, a);
+}
+
+// Ensemble: one CTA per member, each with its own lattice and arguments; the
+// per-step settings are the same for all members.
+struct SqStep {
+    int parity, stages, corr_step, zslot_a, zslot_b;
+};
+template <class S>
+__global__ void __launch_bounds__(SQ_THREADS) k_squirmer_batch(const Lattice* lat, const SqArgs* args, SqStep st) {
+    __shared__ Lattice L;
+    __shared__ SqArgs A;
+    if (threadIdx.x == 0) {
+        L = lat[blockIdx.x];
+        A = args[blockIdx.x];
+        A.parity = st.parity; A.stages = st.stages; A.corr_step = st.corr_step;
+        A.zslot_a = st.zslot_a; A.zslot_b = st.zslot_b;
+    }
+    __syncthreads();
+    squirmer_update<S>(L, A);
 }
 
 }  // namespace lbmgpu

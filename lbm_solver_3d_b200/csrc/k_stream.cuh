@@ -2,14 +2,18 @@
 //  k_stream.cuh -- one time step of LBM::step (src/utils/lbm.cpp:128-224)
 //  over the in-place AA access pattern, as two kernels over disjoint node sets:
 //
-//    k_bulk      every FLUID node with no WALL or PARTICLE neighbour (flag byte
-//                exactly 0). A 3-D grid, threads along x: no integer division,
-//                no neighbour-type lookup, no branch per direction.
-//    k_boundary  the FLUID nodes next to a wall (a static list) and next to the
-//                sphere (the boundary-link list the squirmer kernel rebuilds):
-//                halfway bounce-back with the moving-boundary correction and the
-//                momentum exchange, reduced per node (sphere) or per block
-//                (walls).
+//    k_bulk  every FLUID node without a PARTICLE neighbour outside the zone
+//            around the sphere. A 3-D grid, threads along x: no integer
+//            division, no neighbour-type lookup, nothing read from the
+//            squirmer update. Wall layers are whole x-rows, so a row next to a
+//            wall knows its solid directions from (y, z) alone (halfway
+//            bounce-back, momentum exchange on the wall).
+//    k_zone  the FLUID nodes of the zone (a box of fixed width around the
+//            sphere, see ZoneBox): halfway bounce-back with the moving-boundary
+//            correction and the momentum exchange, reduced per node (sphere)
+//            or per block (walls).
+//  Because k_bulk never touches the zone, it may run while the squirmer update
+//  of the previous step is still remapping the sphere.
 //
 //  Layout: one population array A[i][n] = A[i*N + n] (structure of arrays,
 //  n = x + nx*(y + ny*z)), no second buffer.
@@ -131,118 +135,151 @@ __device__ __forceinline__ void load_node(const typename S::T* __restrict__ f, u
     }
 }
 
-// The per-step settings every thread reads from the device state.
-struct StepFlags {
-    bool do_mass;
-    int corr_on;
-    double corr;
+__device__ __forceinline__ bool in_zone(const Lattice& L, const ZoneBox& z, int x, int y, int zc) {
+    return in_zone_axis(x, z.lo[0], z.w[0], L.nx, false) && in_zone_axis(y, z.lo[1], z.w[1], L.ny, L.walls_y) &&
+           in_zone_axis(zc, z.lo[2], z.w[2], L.nz, L.walls_z);
+}
+
+// Partial sums a node contributes: wall force, stored mass (correction steps),
+// sphere force and torque.
+struct NodeSums {
+    double fw[3] = {0, 0, 0};
+    double mass = 0;
+    double fp[3] = {0, 0, 0}, tp[3] = {0, 0, 0};
 };
-template <bool SQ>
-__device__ __forceinline__ StepFlags step_flags(const StreamArgs& a) {
-    StepFlags s{false, 0, 0.0};
-    if (SQ) {
-        const SqState* sq = a.sq;
-        s.corr_on = sq->corr_pending;
-        s.corr = sq->corr_d;
-        if (a.fused && sq->mass_every > 0) s.do_mass = ((sq->t + 1) % sq->mass_every) == 0;
-    }
-    return s;
-}
-
-__device__ __forceinline__ bool in_rho_box(const Lattice& L, const SqState* sq, int x, int y, int z) {
-    int dx = x - sq->rb_lo[0]; if (dx < 0) dx += L.nx;
-    int dy = y - sq->rb_lo[1]; if (dy < 0) dy += L.ny;
-    int dz = z - sq->rb_lo[2]; if (dz < 0) dz += L.nz;
-    return dx < sq->rb_w[0] && dy < sq->rb_w[1] && dz < sq->rb_w[2];
-}
 
 // ---------------------------------------------------------------------------
-//  k_bulk<S, PAR, SQ, MACRO>: nodes whose flag byte is 0.
-//    SQ    the lattice has a squirmer: store rho inside the refill region,
-//          apply a pending mass correction, sum the mass on correction steps
-//    MACRO store rho and u of every node (the last step of every host call)
-//  grid (ceil(nx/blockDim.x), ny, nz); block (TX, 1, 1) with TX = 32..256.
+//  update_node: the whole LBM::step body for one fluid node n.
+//    GENERAL = false: every neighbour is fluid (flag byte 0): plain push.
+//    GENERAL = true : neighbour types are read for nodes whose flag has a
+//                     near-wall / near-particle bit: bounce-back, momentum
+//                     exchange.
+//    STORE_RHO: keep rho (and u if MACRO) for this node.
 // ---------------------------------------------------------------------------
-template <class S, int PAR, bool SQ, bool MACRO>
-__global__ void __launch_bounds__(256) k_bulk(const Lattice L, const StreamArgs a) {
+// Wall-adjacent rows, for the bulk kernel: bit 0 the y-1 layer is a wall,
+// bit 1 the y+1 layer, bit 2 z-1, bit 3 z+1 (a whole x-row shares them).
+__device__ __forceinline__ uint8_t wall_row(const Lattice& L, int y, int z) {
+    uint8_t w = 0;
+    if (L.walls_y) { if (y == 1) w |= 1; if (y == L.ny - 2) w |= 2; }
+    if (L.walls_z) { if (z == 1) w |= 4; if (z == L.nz - 2) w |= 8; }
+    return w;
+}
+__device__ __forceinline__ bool wall_dir(int i, uint8_t wr) {
+    return (CY(i) < 0 && (wr & 1)) || (CY(i) > 0 && (wr & 2)) || (CZ(i) < 0 && (wr & 4)) || (CZ(i) > 0 && (wr & 8));
+}
+
+template <class S, int PAR, bool GENERAL, bool MACRO>
+__device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
+                                            uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out) {
     using T = typename S::T;
     T* __restrict__ f = static_cast<T*>(a.f);
     const unsigned N = L.N;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
-    const bool active = x < L.nx && a.flag[n] == 0;
-    const StepFlags sf = step_flags<SQ>(a);
-    double msum = 0.0;
+    const Nbr nb(L, x, y, z);
+    // GENERAL: neighbour types from the flag bytes; otherwise only whole wall
+    // layers next to the row (wallrow) can be solid.
+    const bool boundary = GENERAL ? (fl & (NEAR_WALL | NEAR_PARTICLE)) != 0 : wallrow != 0;
+    const SqState* __restrict__ sq = a.sq;
+    const bool do_mass = a.do_mass != 0;
 
-    if (active) {
-        const Nbr nb(L, x, y, z);
-        const bool store_rho = MACRO || (SQ && in_rho_box(L, a.sq, x, y, z));
-        if constexpr (!S::shifted) {
-            // ---------------- FP64: the reference's arithmetic ----------------
-            double fv[Q];
-            load_node<S, PAR>(f, N, n, nb, fv);
-            if (SQ && sf.corr_on) {
+    if constexpr (!S::shifted) {
+        // ---------------- FP64: the reference's arithmetic ----------------
+        double fv[Q];
+        load_node<S, PAR>(f, N, n, nb, fv);
+        if (a.apply_corr) {
+            const double corr = sq->corr_d;
 #pragma unroll
-                for (int i = 0; i < Q; ++i) fv[i] += WD(i) * sf.corr;  // LBM::correctMass (lbm.cpp:337)
-            }
-            // moments, Guo half-force velocity (lbm.cpp:143-152)
-            double r = 0, mx = 0, my = 0, mz = 0;
+            for (int i = 0; i < Q; ++i) fv[i] += WD(i) * corr;  // LBM::correctMass (lbm.cpp:337)
+        }
+        // moments, Guo half-force velocity (lbm.cpp:143-152)
+        double r = 0, mx = 0, my = 0, mz = 0;
 #pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                r += fv[i];
-                if (CX(i) > 0) mx += fv[i]; else if (CX(i) < 0) mx -= fv[i];
-                if (CY(i) > 0) my += fv[i]; else if (CY(i) < 0) my -= fv[i];
-                if (CZ(i) > 0) mz += fv[i]; else if (CZ(i) < 0) mz -= fv[i];
-            }
-            const double Fx = L.F[0], Fy = L.F[1], Fz = L.F[2];
-            const double u = (mx + 0.5 * Fx) / r, v = (my + 0.5 * Fy) / r, wz = (mz + 0.5 * Fz) / r;
-            if (store_rho) a.rho[n] = r;
-            if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-            const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
+        for (int i = 0; i < Q; ++i) {
+            r += fv[i];
+            if (CX(i) > 0) mx += fv[i]; else if (CX(i) < 0) mx -= fv[i];
+            if (CY(i) > 0) my += fv[i]; else if (CY(i) < 0) my -= fv[i];
+            if (CZ(i) > 0) mz += fv[i]; else if (CZ(i) < 0) mz -= fv[i];
+        }
+        const double Fx = L.F[0], Fy = L.F[1], Fz = L.F[2];
+        const double u = (mx + 0.5 * Fx) / r, v = (my + 0.5 * Fy) / r, wz = (mz + 0.5 * Fz) / r;
+        if (store_rho) a.rho[n] = r;
+        if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
+        const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
 #pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                // TRT + Guo forcing (lbm.cpp:162-172)
-                const int io = OPP(i);
-                const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-                const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
-                const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
-                const double feqM = WD(i) * r * 3.0 * cu;
-                const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
-                const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
-                const double fpost = fv[i] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM;
-                S::st(PAR == 0 ? f + (size_t)io * N + n : f + (size_t)i * N + nb.of(n, i), fpost);
-                if (SQ && sf.do_mass) msum += fpost;
+        for (int i = 0; i < Q; ++i) {
+            // TRT + Guo forcing (lbm.cpp:162-172)
+            const int io = OPP(i);
+            const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+            const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
+            const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
+            const double feqM = WD(i) * r * 3.0 * cu;
+            const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
+            const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
+            const double fpost = fv[i] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM;
+            const unsigned nbi = nb.of(n, i);
+            T* local = f + (size_t)io * N + n;
+            T* remote = f + (size_t)i * N + nbi;
+            uint8_t tt = T_FLUID;
+            if (boundary && i != 0) tt = GENERAL ? (a.flag[nbi] & TYPE_MASK) : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
+            if (tt == T_FLUID) {  // push (lbm.cpp:186)
+                S::st(PAR == 0 ? local : remote, fpost);
+                if (do_mass) out.mass += fpost;
+                continue;
             }
-        } else {
-            // ------------- FP32 arithmetic on stored deviations ---------------
-            float d[Q];
-            load_node<S, PAR>(f, N, n, nb, d);
-            if (SQ && sf.corr_on) {
+            // halfway bounce-back with moving-boundary correction (lbm.cpp:189-199)
+            double ub[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
+            if (GENERAL && tt == T_PARTICLE) {
+                offset_from_squirmer(L, sq, x + 0.5 * CX(i), y + 0.5 * CY(i), z + 0.5 * CZ(i), rb);
+                surface_velocity(sq, rb, ub, true);
+            }
+            const double cub = CX(i) * ub[0] + CY(i) * ub[1] + CZ(i) * ub[2];
+            const double fb = fpost - 6.0 * WD(i) * r * cub;
+            S::st(PAR == 0 ? remote : local, fb);
+            if (do_mass) out.mass += fb;
+            // Galilean-invariant momentum exchange (lbm.cpp:202-215)
+            const double sm = fpost + fb, dl = fpost - fb;
+            const double dpx = sm * CX(i) - dl * ub[0];
+            const double dpy = sm * CY(i) - dl * ub[1];
+            const double dpz = sm * CZ(i) - dl * ub[2];
+            if (tt == T_WALL) { out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz; }
+            else {
+                out.fp[0] += dpx; out.fp[1] += dpy; out.fp[2] += dpz;
+                out.tp[0] += rb[1] * dpz - rb[2] * dpy;
+                out.tp[1] += rb[2] * dpx - rb[0] * dpz;
+                out.tp[2] += rb[0] * dpy - rb[1] * dpx;
+            }
+        }
+    } else {
+        // ------------- FP32 arithmetic on stored deviations ---------------
+        float d[Q];
+        load_node<S, PAR>(f, N, n, nb, d);
+        if (a.apply_corr) {
+            const double corr = sq->corr_d;
 #pragma unroll
-                for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * sf.corr);
-            }
-            float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+            for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * corr);
+        }
+        float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                dr += d[i];
-                if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
-                if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
-                if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
-            }
-            const float rho = 1.0f + dr;
-            const float inv = 1.0f / rho;
-            const float u = (jx + 0.5f * L.Ff[0]) * inv, v = (jy + 0.5f * L.Ff[1]) * inv, wz = (jz + 0.5f * L.Ff[2]) * inv;
-            if (store_rho) a.rho[n] = 1.0 + (double)dr;
-            if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-            const float usq = u * u + v * v + wz * wz;
-            const float uF = u * L.Ff[0] + v * L.Ff[1] + wz * L.Ff[2];
-            const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
-            const float k15 = 1.5f * usq;
+        for (int i = 0; i < Q; ++i) {
+            dr += d[i];
+            if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
+            if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
+            if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
+        }
+        const float rho = 1.0f + dr;
+        const float inv = 1.0f / rho;
+        const float u = (jx + 0.5f * L.Ff[0]) * inv, v = (jy + 0.5f * L.Ff[1]) * inv, wz = (jz + 0.5f * L.Ff[2]) * inv;
+        if (store_rho) a.rho[n] = 1.0 + (double)dr;
+        if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
+        const float usq = u * u + v * v + wz * wz;
+        const float uF = u * L.Ff[0] + v * L.Ff[1] + wz * L.Ff[2];
+        const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
+        const float k15 = 1.5f * usq;
+        if (!boundary) {
             {   // rest population: c = 0
                 const float eP = WF(0) * (dr - rho * k15);
-                const float out = d[0] - omP * (d[0] - eP) - gP * WF(0) * 3.0f * uF;
-                S::st(f + n, out);
-                if (SQ && sf.do_mass) msum += (double)S::rt(out);
+                const float o0 = d[0] - omP * (d[0] - eP) - gP * WF(0) * 3.0f * uF;
+                S::st(f + n, o0);
+                if (do_mass) out.mass += (double)S::rt(o0);
             }
 #pragma unroll
             for (int i = 1; i < Q; i += 2) {
@@ -262,140 +299,9 @@ __global__ void __launch_bounds__(256) k_bulk(const Lattice L, const StreamArgs 
                     S::st(f + (size_t)i * N + nb.of(n, i), oi);
                     S::st(f + (size_t)io * N + nb.of(n, io), oo);
                 }
-                if (SQ && sf.do_mass) msum += (double)S::rt(oi) + (double)S::rt(oo);
-            }
-        }
-    }
-    if (SQ && sf.do_mass) {
-        const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-        block_reduce4<256>(0.0, 0.0, 0.0, msum, a.block_part + (size_t)bid * BLOCK_PART);
-    }
-}
-
-// ---------------------------------------------------------------------------
-//  k_boundary<S, PAR, SQ, MACRO>: thread k handles wall_nodes[k] (k < n_wall;
-//  skipped unless FLUID without PARTICLE neighbour) or links[k - n_wall]
-//  (k - n_wall < n_links, the row of link_part it writes).
-// ---------------------------------------------------------------------------
-template <class S, int PAR, bool SQ, bool MACRO>
-__global__ void __launch_bounds__(BOUNDARY_BLOCK) k_boundary(const Lattice L, const StreamArgs a) {
-    using T = typename S::T;
-    T* __restrict__ f = static_cast<T*>(a.f);
-    const unsigned N = L.N;
-    const SqState* __restrict__ sq = a.sq;
-    const int k = blockIdx.x * BOUNDARY_BLOCK + threadIdx.x;
-    const int n_links = SQ ? sq->n_links : 0;
-    int link = -1;
-    unsigned n = 0;
-    bool active = false;
-    if (k < a.n_wall) {
-        n = (unsigned)a.wall_nodes[k];
-        const uint8_t fl = a.flag[n];
-        active = (fl & TYPE_MASK) == T_FLUID && !(fl & NEAR_PARTICLE);
-    } else if (SQ && k - a.n_wall < n_links) {
-        link = k - a.n_wall;
-        n = (unsigned)a.links[link];
-        active = true;
-    }
-    const StepFlags sf = step_flags<SQ>(a);
-    const bool do_red = MACRO || sf.do_mass;
-    double fw0 = 0.0, fw1 = 0.0, fw2 = 0.0, msum = 0.0;
-
-    if (active) {
-        const int x = (int)(n % (unsigned)L.nx);
-        const unsigned yz = n / (unsigned)L.nx;
-        const int y = (int)(yz % (unsigned)L.ny);
-        const int z = (int)(yz / (unsigned)L.ny);
-        const Nbr nb(L, x, y, z);
-        const bool store_rho = MACRO || (SQ && in_rho_box(L, sq, x, y, z));
-        double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0, tp0 = 0.0, tp1 = 0.0, tp2 = 0.0;
-
-        if constexpr (!S::shifted) {
-            double fv[Q];
-            load_node<S, PAR>(f, N, n, nb, fv);
-            if (SQ && sf.corr_on) {
-#pragma unroll
-                for (int i = 0; i < Q; ++i) fv[i] += WD(i) * sf.corr;
-            }
-            double r = 0, mx = 0, my = 0, mz = 0;
-#pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                r += fv[i];
-                if (CX(i) > 0) mx += fv[i]; else if (CX(i) < 0) mx -= fv[i];
-                if (CY(i) > 0) my += fv[i]; else if (CY(i) < 0) my -= fv[i];
-                if (CZ(i) > 0) mz += fv[i]; else if (CZ(i) < 0) mz -= fv[i];
-            }
-            const double Fx = L.F[0], Fy = L.F[1], Fz = L.F[2];
-            const double u = (mx + 0.5 * Fx) / r, v = (my + 0.5 * Fy) / r, wz = (mz + 0.5 * Fz) / r;
-            if (store_rho) a.rho[n] = r;
-            if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-            const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
-#pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                const int io = OPP(i);
-                const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-                const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
-                const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
-                const double feqM = WD(i) * r * 3.0 * cu;
-                const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
-                const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
-                const double fpost = fv[i] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM;
-                const unsigned nbi = nb.of(n, i);
-                T* local = f + (size_t)io * N + n;
-                T* remote = f + (size_t)i * N + nbi;
-                const uint8_t tt = i == 0 ? T_FLUID : (a.flag[nbi] & TYPE_MASK);
-                if (tt == T_FLUID) {  // push (lbm.cpp:186)
-                    S::st(PAR == 0 ? local : remote, fpost);
-                    if (sf.do_mass) msum += fpost;
-                    continue;
-                }
-                // halfway bounce-back with moving-boundary correction (lbm.cpp:189-199)
-                double ub[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
-                if (SQ && tt == T_PARTICLE) {
-                    offset_from_squirmer(L, sq, x + 0.5 * CX(i), y + 0.5 * CY(i), z + 0.5 * CZ(i), rb);
-                    surface_velocity(sq, rb, ub, true);
-                }
-                const double cub = CX(i) * ub[0] + CY(i) * ub[1] + CZ(i) * ub[2];
-                const double fb = fpost - 6.0 * WD(i) * r * cub;
-                S::st(PAR == 0 ? remote : local, fb);
-                if (sf.do_mass) msum += fb;
-                // Galilean-invariant momentum exchange (lbm.cpp:202-215)
-                const double sm = fpost + fb, dl = fpost - fb;
-                const double dpx = sm * CX(i) - dl * ub[0];
-                const double dpy = sm * CY(i) - dl * ub[1];
-                const double dpz = sm * CZ(i) - dl * ub[2];
-                if (tt == T_WALL) { fw0 += dpx; fw1 += dpy; fw2 += dpz; }
-                else {
-                    fp0 += dpx; fp1 += dpy; fp2 += dpz;
-                    tp0 += rb[1] * dpz - rb[2] * dpy;
-                    tp1 += rb[2] * dpx - rb[0] * dpz;
-                    tp2 += rb[0] * dpy - rb[1] * dpx;
-                }
+                if (do_mass) out.mass += (double)S::rt(oi) + (double)S::rt(oo);
             }
         } else {
-            float d[Q];
-            load_node<S, PAR>(f, N, n, nb, d);
-            if (SQ && sf.corr_on) {
-#pragma unroll
-                for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * sf.corr);
-            }
-            float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                dr += d[i];
-                if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
-                if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
-                if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
-            }
-            const float rho = 1.0f + dr;
-            const float inv = 1.0f / rho;
-            const float u = (jx + 0.5f * L.Ff[0]) * inv, v = (jy + 0.5f * L.Ff[1]) * inv, wz = (jz + 0.5f * L.Ff[2]) * inv;
-            if (store_rho) a.rho[n] = 1.0 + (double)dr;
-            if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-            const float usq = u * u + v * v + wz * wz;
-            const float uF = u * L.Ff[0] + v * L.Ff[1] + wz * L.Ff[2];
-            const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
-            const float k15 = 1.5f * usq;
             float post[Q];
             post[0] = d[0] - omP * (d[0] - WF(0) * (dr - rho * k15)) - gP * WF(0) * 3.0f * uF;
 #pragma unroll
@@ -417,14 +323,15 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_boundary(const Lattice L, co
                 const unsigned nbi = nb.of(n, i);
                 T* local = f + (size_t)OPP(i) * N + n;
                 T* remote = f + (size_t)i * N + nbi;
-                const uint8_t tt = i == 0 ? T_FLUID : (a.flag[nbi] & TYPE_MASK);
+                const uint8_t tt = i == 0 ? T_FLUID
+                                   : GENERAL ? (a.flag[nbi] & TYPE_MASK) : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
                 if (tt == T_FLUID) {
                     S::st(PAR == 0 ? local : remote, dpost);
-                    if (sf.do_mass) msum += (double)S::rt(dpost);
+                    if (do_mass) out.mass += (double)S::rt(dpost);
                     continue;
                 }
                 double ub[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
-                if (SQ && tt == T_PARTICLE) {
+                if (GENERAL && tt == T_PARTICLE) {
                     offset_from_squirmer(L, sq, x + 0.5 * CX(i), y + 0.5 * CY(i), z + 0.5 * CZ(i), rb);
                     surface_velocity(sq, rb, ub, true);
                 }
@@ -432,27 +339,95 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_boundary(const Lattice L, co
                 const double dl = 6.0 * WD(i) * (double)rho * cub;   // fpost - fb
                 const float dfb = (float)((double)dpost - dl);
                 S::st(PAR == 0 ? remote : local, dfb);
-                if (sf.do_mass) msum += (double)S::rt(dfb);
+                if (do_mass) out.mass += (double)S::rt(dfb);
                 const double fpost = WD(i) + (double)dpost;
                 const double sm = 2.0 * fpost - dl;                   // fpost + fb
                 const double dpx = sm * CX(i) - dl * ub[0];
                 const double dpy = sm * CY(i) - dl * ub[1];
                 const double dpz = sm * CZ(i) - dl * ub[2];
-                if (tt == T_WALL) { fw0 += dpx; fw1 += dpy; fw2 += dpz; }
+                if (tt == T_WALL) { out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz; }
                 else {
-                    fp0 += dpx; fp1 += dpy; fp2 += dpz;
-                    tp0 += rb[1] * dpz - rb[2] * dpy;
-                    tp1 += rb[2] * dpx - rb[0] * dpz;
-                    tp2 += rb[0] * dpy - rb[1] * dpx;
+                    out.fp[0] += dpx; out.fp[1] += dpy; out.fp[2] += dpz;
+                    out.tp[0] += rb[1] * dpz - rb[2] * dpy;
+                    out.tp[1] += rb[2] * dpx - rb[0] * dpz;
+                    out.tp[2] += rb[0] * dpy - rb[1] * dpx;
                 }
             }
         }
-        if (SQ && link >= 0) {
-            double* lp = a.link_part + (size_t)link * LINK_PART;
-            lp[0] = fp0; lp[1] = fp1; lp[2] = fp2; lp[3] = tp0; lp[4] = tp1; lp[5] = tp2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+//  k_bulk<S, PAR, SQ, MACRO, WR>: fluid nodes without a PARTICLE neighbour,
+//  outside the zone.
+//    SQ    the lattice has a squirmer (and hence a zone to skip)
+//    MACRO store rho and u of every node (the last step of every host call)
+//    WR    false: grid (ceil(nx/TX), ny, nz), rows next to a wall skipped;
+//          true : grid (ceil(nx/TX), n_wallrows), only those rows, whose
+//                 solid directions follow from (y, z) (bounce-back and the
+//                 wall's momentum exchange compiled in only here)
+//  block (TX, 1, 1) with TX = 32..256. Block partials are indexed by the row,
+//  so the two launches fill disjoint entries of one array. Reads nothing the
+//  squirmer update writes (except the correction value on the step after a
+//  correction step, when the launch waits for it).
+// ---------------------------------------------------------------------------
+template <class S, int PAR, bool SQ, bool MACRO, bool WR>
+__global__ void __launch_bounds__(256, S::shifted ? 4 : 2) k_bulk(const Lattice L, const StreamArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y, z;
+    if (WR) { y = a.wallrows[2 * blockIdx.y]; z = a.wallrows[2 * blockIdx.y + 1]; }
+    else { y = blockIdx.y; z = blockIdx.z; }
+    const uint8_t wr = wall_row(L, y, z);
+    if (!WR && wr) return;  // block-uniform: the wall-row launch owns this row and its partials
+    const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+    // FLUID with no PARTICLE neighbour; wall neighbours are whole layers
+    bool active = x < L.nx && (a.flag[n] & (uint8_t)~NEAR_WALL) == 0;
+    if (SQ && active) active = !in_zone(L, a.sq->zone[a.zslot], x, y, z);
+    NodeSums sums;
+    if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, WR ? wr : (uint8_t)0, MACRO, sums);
+    if (a.do_mass || MACRO) {
+        const unsigned bid = blockIdx.x + gridDim.x * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+        block_reduce4<256>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass, a.block_part + (size_t)bid * BLOCK_PART);
+    }
+}
+
+// ---------------------------------------------------------------------------
+//  k_zone<S, PAR, SQ, MACRO>: thread k updates the fluid node at cell k of the
+//  zone (row-major, x fastest). Zone nodes store rho every step (the refill of
+//  the next remap reads it) and write one row of link_part per near-particle
+//  node; wall force and mass go to block partials.
+// ---------------------------------------------------------------------------
+template <class S, int PAR, bool SQ, bool MACRO>
+__global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
+    const int k = blockIdx.x * BOUNDARY_BLOCK + threadIdx.x;
+    bool active = false;
+    unsigned n = 0;
+    int x = 0, y = 0, z = 0;
+    const ZoneBox* zb = SQ ? &a.sq->zone[a.zslot] : nullptr;
+    if (SQ && k < a.zone_cells) {
+        const int bx = k % a.zw[0], by = (k / a.zw[0]) % a.zw[1], bz = k / (a.zw[0] * a.zw[1]);
+        x = zb->lo[0] + bx; if (x >= L.nx) x -= L.nx;
+        y = zb->lo[1] + by; z = zb->lo[2] + bz;
+        if (L.walls_y) active = y >= 0 && y < L.ny; else { if (y >= L.ny) y -= L.ny; active = true; }
+        if (L.walls_z) active = active && z >= 0 && z < L.nz; else if (z >= L.nz) z -= L.nz;
+        if (active) {
+            n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+            active = (a.flag[n] & TYPE_MASK) == T_FLUID;
         }
     }
-    if (do_red) block_reduce4<BOUNDARY_BLOCK>(fw0, fw1, fw2, msum, a.block_part_b + (size_t)blockIdx.x * BLOCK_PART);
+    NodeSums sums;
+    if (active) {
+        const uint8_t fl = a.flag[n];
+        update_node<S, PAR, true, MACRO>(L, a, n, x, y, z, fl, 0, SQ || MACRO, sums);
+        if (SQ && (fl & NEAR_PARTICLE)) {
+            double* lp = a.link_part + (size_t)a.linkslot[n] * LINK_PART;
+            lp[0] = sums.fp[0]; lp[1] = sums.fp[1]; lp[2] = sums.fp[2];
+            lp[3] = sums.tp[0]; lp[4] = sums.tp[1]; lp[5] = sums.tp[2];
+        }
+    }
+    if (MACRO || a.do_mass)
+        block_reduce4<BOUNDARY_BLOCK>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass,
+                                      a.block_part_b + (size_t)blockIdx.x * BLOCK_PART);
 }
 
 }  // namespace lbmgpu

@@ -12,17 +12,22 @@ namespace lbmgpu {
 
 struct SqArgs;
 
-// launch geometry of one step: the bulk kernel's 3-D grid and the boundary
-// kernel's 1-D grid (0: no boundary nodes)
+// launch geometry of one step: the bulk kernel's 3-D grid and the zone
+// kernel's 1-D grid (0: no zone and no wall nodes)
 struct StreamGeom {
     dim3 grid, block;
     unsigned bgrid;
+    unsigned nwallrows;  // rows next to a wall (0: none)
 };
 
 struct Launchers {
-    // one time step of the collide-stream kernels (bulk + boundary)
-    void (*stream)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
-                   cudaStream_t st);
+    // the two collide-stream kernels of one time step
+    void (*bulk)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
+                 cudaStream_t st);
+    void (*wallrows)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
+                     cudaStream_t st);
+    void (*zone)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
+                 cudaStream_t st);
     // the squirmer update (stages: STAGE_* bits)
     void (*squirmer)(const Lattice& L, const SqArgs& a, cudaStream_t st);
     void (*fill_rest)(const Lattice& L, void* f, cudaStream_t st);

@@ -3,6 +3,7 @@
 //  device-side records shared by the kernels of liblbmgpu.
 // ============================================================================
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_fp16.h>
 
@@ -85,6 +86,39 @@ struct Lattice {
     float cF[Q], cm[Q];
 };
 
+// ---- the zone around the sphere ----------------------------------------------
+// A box of fixed width around the sphere. Its fluid nodes are updated by the
+// zone kernel, which runs after the squirmer update of the previous step; the
+// bulk kernel skips them and so need not wait for that update. lo is the
+// lower corner (unwrapped along y/z walls, wrapped into [0, n) along periodic
+// axes); w the width actually covered (at most the lattice extent). Zones are
+// kept for three consecutive steps (slot = step mod 3): the squirmer update of
+// step s writes the zone of step s + 2 while steps s + 1 read theirs.
+struct ZoneBox {
+    int lo[3], w[3];
+};
+constexpr int ZONE_SLOTS = 3;
+constexpr int ZONE_MARGIN = 4;  // cells around the remap box (see k_squirmer.cuh)
+
+// Zone width along an axis: the remap box (lbm.cpp:273-275) is at most
+// 2*ceil(R) + 6 cells wide; the zone adds ZONE_MARGIN cells on each side.
+__host__ __device__ inline int zone_width(double R, int n, bool wall_axis) {
+    const int w = 2 * (int)ceil(R) + 6 + 2 * ZONE_MARGIN;
+    return wall_axis ? w : (w < n ? w : n);
+}
+
+// The zone around remap box [blo, blo + bw) along one axis.
+__host__ __device__ inline void zone_axis(int blo, int n, int w, bool wall_axis, int& lo) {
+    lo = blo - ZONE_MARGIN;
+    if (!wall_axis) lo = w >= n ? 0 : ((lo % n) + n) % n;
+}
+
+__host__ __device__ inline bool in_zone_axis(int c, int lo, int w, int n, bool wall_axis) {
+    int d = c - lo;
+    if (!wall_axis && d < 0) d += n;
+    return d >= 0 && d < w;
+}
+
 // ---- squirmer / run state on the device ------------------------------------
 // Everything the per-step kernels need to decide and compute without a host
 // round trip. FP64 throughout.
@@ -102,9 +136,8 @@ struct SqState {
     int mass_every, traj_every;
     int corr_pending;            // apply f_i += w_i * corr_d on the next load
     double corr_d;
-    // region of nodes whose rho the next step must store (for the refill)
-    int rb_lo[3], rb_w[3];       // wrapped lower corner, width (<= extent)
-    int rb_valid;
+    // zones of the next steps (slot = step mod 3)
+    ZoneBox zone[ZONE_SLOTS];
     // boundary-link list
     int n_links;
     // last wall force (written on macro steps)
@@ -129,13 +162,18 @@ struct StreamArgs {
     double* rho;                  // pre-collision moments (FP64)
     double* ux; double* uy; double* uz;
     double* link_part;            // [n_links][LINK_PART], one row per near-particle node
+    const int* linkslot;          // node -> its row of link_part
     double* block_part;           // bulk kernel: [blocks][BLOCK_PART]
-    double* block_part_b;         // boundary kernel: [blocks][BLOCK_PART]
-    const int* wall_nodes;        // static list: non-wall nodes with a WALL neighbour
-    int n_wall;
-    const int* links;             // boundary-link list (near-particle nodes)
+    double* block_part_b;         // zone kernel: [blocks][BLOCK_PART]
+    const int* wallrows;          // (y, z) of the fluid rows next to a wall
+    int n_wallrows;
+    int zone_cells;               // cells of the zone grid (zone width product bound)
+    int zw[3];                    // zone grid extents (fixed per lattice)
     SqState* sq;
-    int fused;                    // 1: time-loop mode (mass sums on correction steps)
+    // per-step settings, fixed at launch (hence in a captured graph):
+    int zslot;                    // zone slot of this step
+    int do_mass;                  // sum the stored populations (a correction step)
+    int apply_corr;               // add the pending correction on load (after one)
 };
 
 }  // namespace lbmgpu

@@ -11,26 +11,37 @@
 namespace lbmgpu {
 
 template <class S, int PAR, bool SQ, bool MACRO>
-static void stream_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
-    k_bulk<S, PAR, SQ, MACRO><<<g.grid, g.block, 0, st>>>(L, a);
-    if (g.bgrid) k_boundary<S, PAR, SQ, MACRO><<<g.bgrid, BOUNDARY_BLOCK, 0, st>>>(L, a);
+static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    k_bulk<S, PAR, SQ, MACRO, false><<<g.grid, g.block, 0, st>>>(L, a);
+}
+template <class S, int PAR, bool SQ, bool MACRO>
+static void wallrows_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if (g.nwallrows) k_bulk<S, PAR, SQ, MACRO, true><<<dim3(g.grid.x, g.nwallrows, 1), g.block, 0, st>>>(L, a);
+}
+template <class S, int PAR, bool SQ, bool MACRO>
+static void zone_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if (g.bgrid) k_zone<S, PAR, SQ, MACRO><<<g.bgrid, BOUNDARY_BLOCK, 0, st>>>(L, a);
 }
 
-template <class S>
-static void stream_dispatch(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& grid,
-                            cudaStream_t st) {
-    const int key = (par ? 4 : 0) | (sq ? 2 : 0) | (macro ? 1 : 0);
-    switch (key) {
-        case 0: stream_one<S, 0, false, false>(L, a, grid, st); break;
-        case 1: stream_one<S, 0, false, true>(L, a, grid, st); break;
-        case 2: stream_one<S, 0, true, false>(L, a, grid, st); break;
-        case 3: stream_one<S, 0, true, true>(L, a, grid, st); break;
-        case 4: stream_one<S, 1, false, false>(L, a, grid, st); break;
-        case 5: stream_one<S, 1, false, true>(L, a, grid, st); break;
-        case 6: stream_one<S, 1, true, false>(L, a, grid, st); break;
-        default: stream_one<S, 1, true, true>(L, a, grid, st); break;
+#define LBMGPU_DISPATCH(FN)                                                                                  \
+    template <class S>                                                                                       \
+    static void FN##_dispatch(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a,          \
+                              const StreamGeom& g, cudaStream_t st) {                                        \
+        switch ((par ? 4 : 0) | (sq ? 2 : 0) | (macro ? 1 : 0)) {                                            \
+            case 0: FN##_one<S, 0, false, false>(L, a, g, st); break;                                        \
+            case 1: FN##_one<S, 0, false, true>(L, a, g, st); break;                                         \
+            case 2: FN##_one<S, 0, true, false>(L, a, g, st); break;                                         \
+            case 3: FN##_one<S, 0, true, true>(L, a, g, st); break;                                          \
+            case 4: FN##_one<S, 1, false, false>(L, a, g, st); break;                                        \
+            case 5: FN##_one<S, 1, false, true>(L, a, g, st); break;                                         \
+            case 6: FN##_one<S, 1, true, false>(L, a, g, st); break;                                         \
+            default: FN##_one<S, 1, true, true>(L, a, g, st); break;                                         \
+        }                                                                                                    \
     }
-}
+LBMGPU_DISPATCH(bulk)
+LBMGPU_DISPATCH(wallrows)
+LBMGPU_DISPATCH(zone)
+#undef LBMGPU_DISPATCH
 
 inline size_t squirmer_smem() { return sizeof(ChgSh) * SQ_BATCH; }
 
@@ -71,7 +82,9 @@ static cudaError_t prepare_launch() {
 template <class S>
 static Launchers make_launchers() {
     Launchers l;
-    l.stream = &stream_dispatch<S>;
+    l.bulk = &bulk_dispatch<S>;
+    l.wallrows = &wallrows_dispatch<S>;
+    l.zone = &zone_dispatch<S>;
     l.squirmer = &squirmer_launch<S>;
     l.fill_rest = &fill_launch<S>;
     l.get_pop = &get_pop_launch<S>;

@@ -2,6 +2,19 @@
 //  lbmgpu.cu -- the C ABI (include/lbmgpu.h): handle, device memory, set-up
 //  of the initial state, the CUDA-graph time loop and the host-facing
 //  accessors.
+//
+//  Time loop (lbmgpu_run). Step s runs three kernels:
+//    B(s)  k_bulk     every fluid node outside the zone (wall rows included)
+//    Z(s)  k_zone     the zone around the sphere
+//    S(s)  k_squirmer rigid body, remap, link list, bookkeeping
+//  on two streams, with exactly the dependencies the data needs:
+//    B(s) after B(s-1), Z(s-1)          [+ S(s-1) if step s-1 was a mass-
+//                                         correction step: B applies it]
+//    Z(s) after B(s-1), Z(s-1), S(s-1)
+//    S(s) after Z(s)                    [+ B(s) on correction steps: mass sums]
+//  so S(s) overlaps B(s+1). Runs of steps are captured once into a CUDA graph
+//  (the pattern repeats with period lcm(2, 3, k): AA parity, zone slot, mass
+//  correction every k steps) and replayed.
 // ============================================================================
 #include <cuda_runtime.h>
 
@@ -9,7 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -23,14 +36,16 @@ using namespace lbmgpu;
 namespace {
 
 constexpr double PI = 3.14159265358979323846;
-constexpr int GRAPH_LONG = 64;   // steps in the long captured graph (even)
 constexpr int DIAG_GRID = 296;
+constexpr int MAX_PERIOD = 240;   // longest correction period captured in one graph pattern
+constexpr int MIN_GRAPH = 48;     // steps per captured graph, at least
 
 thread_local std::string g_create_error;
 
-struct GraphSlot {
+struct Graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int steps = 0;
 };
 
 }  // namespace
@@ -41,22 +56,24 @@ struct lbmgpu_handle {
     const Launchers* lz = nullptr;
     size_t esize = 8;
     int has_sq = 0;
-    cudaStream_t own = nullptr, stream = nullptr, cap = nullptr;
+    cudaStream_t own = nullptr, stream = nullptr;  // the caller-facing stream
+    cudaStream_t zs = nullptr;                     // zone/squirmer stream (high priority)
+    cudaStream_t cap = nullptr, cap2 = nullptr;    // graph capture streams
+    cudaEvent_t ev_b[2] = {nullptr, nullptr}, ev_z = nullptr, ev_s = nullptr, ev_fork = nullptr, ev_join = nullptr;
 
     // device memory
     void* f = nullptr;
     uint8_t* flag = nullptr;
     double *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr;
-    int* wall_nodes = nullptr;
-    int n_wall = 0;
+    int* wallrows = nullptr;     // (y, z) pairs of rows next to a wall
     int* links = nullptr;
+    int* linkslot = nullptr;
     int link_cap = 0;
     double* link_part = nullptr;
     double* block_part = nullptr;
     unsigned nblocks = 0;
     double* block_part_b = nullptr;
     unsigned nblocks_b = 0;
-    StreamGeom geom{};
     int* ordermap = nullptr;
     int* chg_node = nullptr;
     int* chg_key = nullptr;
@@ -66,13 +83,20 @@ struct lbmgpu_handle {
     double* traj = nullptr;
     SqState* sq = nullptr;
     double* scratch = nullptr;   // N doubles
-    double* small = nullptr;     // reduction partials / results (2*MASS_GRID + DIAG_GRID*4 + 16)
+    double* small = nullptr;     // reduction partials / results
+
+    // launch geometry
+    StreamGeom geom{};
+    int zone_cells = 0, zw[3] = {0, 0, 0};
+    int period = 6;              // steps after which the launch pattern repeats
+    bool corr_in_graph = false;  // correction steps are part of the captured pattern
 
     // host mirrors
-    long long t_main = 0;        // stream-kernel steps issued (AA parity)
+    long long t_main = 0;        // time steps issued (AA parity; step s = t_main + 1)
     long long traj_read = 0;
     long long launches = 0;
-    GraphSlot g_short, g_long;
+    bool pending_corr = false;   // a correction computed by the last step is still to be applied
+    Graph g;
     std::string err;
 };
 
@@ -84,12 +108,12 @@ int fail(lbmgpu_handle* h, int code, const std::string& msg) {
     return code;
 }
 
-#define CUDA_TRY(h, call)                                                              \
-    do {                                                                               \
-        cudaError_t e_ = (call);                                                       \
-        if (e_ != cudaSuccess)                                                         \
-            return fail(h, e_ == cudaErrorMemoryAllocation ? LBMGPU_ERR_NOMEM : LBMGPU_ERR_CUDA, \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));           \
+#define CUDA_TRY(h, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? LBMGPU_ERR_NOMEM : LBMGPU_ERR_CUDA,    \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
     } while (0)
 
 const Launchers* launchers_for(int prec) {
@@ -103,23 +127,44 @@ const Launchers* launchers_for(int prec) {
 
 size_t esize_for(int prec) { return prec == LBMGPU_FP64 ? 8 : (prec == LBMGPU_FP32 ? 4 : 2); }
 
-StreamArgs stream_args(lbmgpu_handle* h, int fused) {
+// Settings of time step s (1-based).
+struct StepPlan {
+    long long s;
+    int par, zslot;
+    bool corr;        // s is a mass-correction step
+    bool apply;       // s applies the correction computed by step s - 1
+    bool macro;       // s stores all macroscopic fields and the wall force
+};
+
+bool is_corr_step(const lbmgpu_handle* h, long long s) {
+    const int k = h->p.mass_correction_every;
+    return h->has_sq && k > 0 && s % k == 0;
+}
+
+StreamArgs stream_args(lbmgpu_handle* h, const StepPlan& sp) {
     StreamArgs a;
     a.f = h->f; a.flag = h->flag; a.rho = h->rho; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz;
-    a.link_part = h->link_part; a.block_part = h->block_part; a.block_part_b = h->block_part_b;
-    a.wall_nodes = h->wall_nodes; a.n_wall = h->n_wall; a.links = h->links; a.sq = h->sq;
-    a.fused = fused;
+    a.link_part = h->link_part; a.linkslot = h->linkslot;
+    a.block_part = h->block_part; a.block_part_b = h->block_part_b;
+    a.wallrows = h->wallrows; a.n_wallrows = (int)h->geom.nwallrows;
+    a.zone_cells = h->zone_cells;
+    for (int d = 0; d < 3; ++d) a.zw[d] = h->zw[d];
+    a.sq = h->sq;
+    a.zslot = sp.zslot; a.do_mass = sp.corr ? 1 : 0; a.apply_corr = sp.apply ? 1 : 0;
     return a;
 }
 
-SqArgs squirmer_args(lbmgpu_handle* h, int parity, int stages) {
+SqArgs squirmer_args(lbmgpu_handle* h, int parity, int stages, int corr_step, int za, int zb) {
     SqArgs a;
     a.f = h->f; a.flag = h->flag; a.rho = h->rho; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz;
-    a.links = h->links; a.link_cap = h->link_cap;
+    a.links = h->links; a.linkslot = h->linkslot; a.link_cap = h->link_cap;
     a.link_part = h->link_part; a.block_part = h->block_part; a.nblocks = (int)h->nblocks;
     a.block_part_b = h->block_part_b; a.nblocks_b = (int)h->nblocks_b;
-    a.ordermap = h->ordermap; a.chg_node = h->chg_node; a.chg_key = h->chg_key; a.cand = h->cand; a.mark = h->mark; a.chg_cap = h->chg_cap;
+    a.block_part_w = nullptr; a.nblocks_w = 0;
+    a.ordermap = h->ordermap; a.chg_node = h->chg_node; a.chg_key = h->chg_key; a.cand = h->cand; a.mark = h->mark;
+    a.chg_cap = h->chg_cap;
     a.traj = h->traj; a.sq = h->sq; a.parity = parity; a.stages = stages;
+    a.corr_step = corr_step; a.zslot_a = za; a.zslot_b = zb;
     return a;
 }
 
@@ -130,15 +175,17 @@ __global__ void k_fill_d(double* p, size_t n, double v) {
 __global__ void k_fill_i(int* p, size_t n, int v) {
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) p[k] = v;
 }
+__global__ void k_scatter_slots(const int* links, int n, int* linkslot) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) linkslot[links[k]] = k;
+}
 
-// wall force of a macro step: fixed-order sum of the stream kernel's block partials
-__global__ void k_finalize(const double* block_part, unsigned nblocks, SqState* sq) {
+// wall force of a macro step: fixed-order sum of both kernels' block partials
+__global__ void k_finalize(const double* bp, unsigned nb, const double* bpz, unsigned nbz, SqState* sq) {
     __shared__ double red[8][3];
     double a0 = 0, a1 = 0, a2 = 0;
-    for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x) {
-        a0 += block_part[(size_t)b * BLOCK_PART + 0];
-        a1 += block_part[(size_t)b * BLOCK_PART + 1];
-        a2 += block_part[(size_t)b * BLOCK_PART + 2];
+    for (unsigned b = threadIdx.x; b < nb + nbz; b += blockDim.x) {
+        const double* q = b < nb ? bp + (size_t)b * BLOCK_PART : bpz + (size_t)(b - nb) * BLOCK_PART;
+        a0 += q[0]; a1 += q[1]; a2 += q[2];
     }
     for (int o = 16; o > 0; o >>= 1) {
         a0 += __shfl_down_sync(0xffffffffu, a0, o);
@@ -195,7 +242,7 @@ __global__ void k_diag_final(const double* part, int nparts, double* out) {
 struct HostInit {
     std::vector<uint8_t> flag;
     std::vector<int> links;
-    std::vector<int> wall_nodes;
+    std::vector<int> wallrows;
     SqState s{};
 };
 
@@ -208,6 +255,7 @@ void h_offset(const lbmgpu_params& p, const SqState& s, double px, double py, do
     r[2] = pz - s.X[2]; if (!p.walls_z) r[2] -= p.nz * std::round(r[2] / p.nz);
 }
 
+// the sphere's bounding box (lbm.cpp:272-276)
 void h_box(const lbmgpu_params& p, const SqState& s, int lo[3], int w[3]) {
     const double R = s.R;
     int x0 = (int)std::floor(s.X[0] - R) - 2, x1 = (int)std::ceil(s.X[0] + R) + 2;
@@ -218,16 +266,38 @@ void h_box(const lbmgpu_params& p, const SqState& s, int lo[3], int w[3]) {
     w[0] = x1 - x0 + 1; w[1] = y1 - y0 + 1; w[2] = z1 - z0 + 1;
 }
 
-void build_initial(const lbmgpu_params& p, const Lattice& L, HostInit& hi) {
+void set_zones(const lbmgpu_params& p, SqState& s) {
+    int lo[3], w[3];
+    h_box(p, s, lo, w);
+    const int nd[3] = {p.nx, p.ny, p.nz};
+    const bool wall_axis[3] = {false, p.walls_y != 0, p.walls_z != 0};
+    for (int k = 0; k < ZONE_SLOTS; ++k)
+        for (int d = 0; d < 3; ++d) {
+            s.zone[k].w[d] = zone_width(s.R, nd[d], wall_axis[d]);
+            zone_axis(lo[d], nd[d], s.zone[k].w[d], wall_axis[d], s.zone[k].lo[d]);
+        }
+}
+
+bool near_wall(const lbmgpu_params& p, int y, int z) {
+    return (p.walls_y && (y == 1 || y == p.ny - 2)) || (p.walls_z && (z == 1 || z == p.nz - 2));
+}
+bool is_wall(const lbmgpu_params& p, int y, int z) {
+    return (p.walls_y && (y == 0 || y == p.ny - 1)) || (p.walls_z && (z == 0 || z == p.nz - 1));
+}
+
+void build_initial(const lbmgpu_params& p, HostInit& hi) {
     const size_t N = (size_t)p.nx * p.ny * p.nz;
     hi.flag.assign(N, T_FLUID);
-    // WALL layers (lbm.cpp:72-78)
+    // WALL layers (lbm.cpp:72-78), near-wall bits and the static wall list:
+    // a whole x-row shares its (y, z) classification.
+    long long nf = 0;
     for (int z = 0; z < p.nz; ++z)
-        for (int y = 0; y < p.ny; ++y)
-            for (int x = 0; x < p.nx; ++x) {
-                const bool wall = (p.walls_y && (y == 0 || y == p.ny - 1)) || (p.walls_z && (z == 0 || z == p.nz - 1));
-                hi.flag[hidx(p, x, y, z)] = wall ? T_WALL : T_FLUID;
-            }
+        for (int y = 0; y < p.ny; ++y) {
+            const uint8_t v = is_wall(p, y, z) ? T_WALL : (near_wall(p, y, z) ? (uint8_t)(T_FLUID | NEAR_WALL) : T_FLUID);
+            std::memset(hi.flag.data() + hidx(p, 0, y, z), v, p.nx);
+            if (v != T_WALL) nf += p.nx;
+            if (v == (T_FLUID | NEAR_WALL)) { hi.wallrows.push_back(y); hi.wallrows.push_back(z); }
+        }
     SqState& s = hi.s;
     std::memset(&s, 0, sizeof(s));
     s.present = p.squirmer;
@@ -259,54 +329,35 @@ void build_initial(const lbmgpu_params& p, const Lattice& L, HostInit& hi) {
                 for (int xx = lo[0]; xx < lo[0] + w[0]; ++xx) {
                     const int x = ((xx % p.nx) + p.nx) % p.nx, y = ((yy % p.ny) + p.ny) % p.ny, z = ((zz % p.nz) + p.nz) % p.nz;
                     const size_t n = hidx(p, x, y, z);
-                    if (hi.flag[n] == T_WALL) continue;
+                    if ((hi.flag[n] & TYPE_MASK) == T_WALL) continue;
                     double r[3];
                     h_offset(p, s, x, y, z, r);
                     const bool inside = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < s.R * s.R;
-                    hi.flag[n] = inside ? T_PARTICLE : T_FLUID;
+                    if (inside && (hi.flag[n] & TYPE_MASK) != T_PARTICLE) { hi.flag[n] = T_PARTICLE; --nf; }
                 }
-        const int nd[3] = {p.nx, p.ny, p.nz};
-        for (int d = 0; d < 3; ++d) {
-            const int ww = w[d] + 4;
-            s.rb_w[d] = std::min(ww, nd[d]);
-            s.rb_lo[d] = ww >= nd[d] ? 0 : (((lo[d] - 2) % nd[d]) + nd[d]) % nd[d];
-        }
-        s.rb_valid = 1;
+        // near-particle bits and the boundary-link list (ascending node order):
+        // fluid nodes with a PARTICLE neighbour lie within the box
+        std::vector<int> cand;
+        for (int zz = lo[2] - 1; zz <= lo[2] + w[2]; ++zz)
+            for (int yy = lo[1] - 1; yy <= lo[1] + w[1]; ++yy)
+                for (int xx = lo[0] - 1; xx <= lo[0] + w[0]; ++xx) {
+                    const int x = ((xx % p.nx) + p.nx) % p.nx, y = ((yy % p.ny) + p.ny) % p.ny, z = ((zz % p.nz) + p.nz) % p.nz;
+                    const size_t n = hidx(p, x, y, z);
+                    if ((hi.flag[n] & TYPE_MASK) != T_FLUID) continue;
+                    bool np = false;
+                    for (int i = 1; i < Q && !np; ++i) {
+                        const int xn = (x + CX(i) + p.nx) % p.nx, yn = (y + CY(i) + p.ny) % p.ny, zn = (z + CZ(i) + p.nz) % p.nz;
+                        np = (hi.flag[hidx(p, xn, yn, zn)] & TYPE_MASK) == T_PARTICLE;
+                    }
+                    if (np) cand.push_back((int)n);
+                }
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        for (int n : cand) { hi.flag[n] |= NEAR_PARTICLE; hi.links.push_back(n); }
+        set_zones(p, s);
     }
-    // near-wall / near-particle bits, boundary-link list in node order, fluid count
-    long long nf = 0;
-    std::vector<uint8_t> base(hi.flag);
-    for (int z = 0; z < p.nz; ++z)
-        for (int y = 0; y < p.ny; ++y)
-            for (int x = 0; x < p.nx; ++x) {
-                const size_t n = hidx(p, x, y, z);
-                if (base[n] != T_FLUID) continue;
-                ++nf;
-                bool nw = false, np = false;
-                for (int i = 1; i < Q; ++i) {
-                    const int xn = (x + CX(i) + p.nx) % p.nx, yn = (y + CY(i) + p.ny) % p.ny, zn = (z + CZ(i) + p.nz) % p.nz;
-                    const uint8_t t = base[hidx(p, xn, yn, zn)];
-                    nw |= t == T_WALL; np |= t == T_PARTICLE;
-                }
-                hi.flag[n] = T_FLUID | (nw ? NEAR_WALL : 0) | (np ? NEAR_PARTICLE : 0);
-                if (np) hi.links.push_back((int)n);
-            }
-    // positions next to a wall (static; whatever their type becomes later)
-    for (int z = 0; z < p.nz; ++z)
-        for (int y = 0; y < p.ny; ++y)
-            for (int x = 0; x < p.nx; ++x) {
-                const size_t n = hidx(p, x, y, z);
-                if (base[n] == T_WALL) continue;
-                bool nw = false;
-                for (int i = 1; i < Q; ++i) {
-                    const int xn = (x + CX(i) + p.nx) % p.nx, yn = (y + CY(i) + p.ny) % p.ny, zn = (z + CZ(i) + p.nz) % p.nz;
-                    nw |= base[hidx(p, xn, yn, zn)] == T_WALL;
-                }
-                if (nw) hi.wall_nodes.push_back((int)n);
-            }
     s.n_fluid = nf;
     s.n_links = (int)hi.links.size();
-    (void)L;
 }
 
 int validate_impl(const lbmgpu_params* p, std::string& m) {
@@ -321,6 +372,7 @@ int validate_impl(const lbmgpu_params* p, std::string& m) {
     if (p->traj_every < 1) return bad("print_every and traj_every must be >= 1");
     // additions
     if ((double)p->nx * p->ny * p->nz >= 2147483648.0) return bad("lattice too large: nx*ny*nz must be < 2^31");
+    if (p->ny > 65535 || p->nz > 65535) return bad("ny and nz must be <= 65535");
     if (p->precision < LBMGPU_FP64 || p->precision > LBMGPU_FP16) return bad("precision must be FP64, FP32 or FP16");
     if (p->mass_correction_every < 0) return bad("mass_correction_every must be >= 0");
     if (p->use_orientation && std::sqrt(p->ex * p->ex + p->ey * p->ey + p->ez * p->ez) == 0.0)
@@ -336,44 +388,100 @@ int validate_impl(const lbmgpu_params* p, std::string& m) {
     if (2.0 * p->radius + 2.0 > p->nx || (!p->walls_y && 2.0 * p->radius + 2.0 > p->ny) || 2.0 * p->radius + 2.0 > p->nz)
         return bad("domain too small for the squirmer");
     if (2.0 * p->b1 / 3.0 > 0.05) return bad("swimming speed U0 = 2 B1 / 3 too large (Mach number); keep U0 < 0.05");
+    if (p->radius > 200.0) return bad("squirmer radius must be <= 200 lattice units");
     return LBMGPU_OK;
 }
 
-void free_all(lbmgpu_handle* h) {
-    for (GraphSlot* g : {&h->g_short, &h->g_long}) {
-        if (g->exec) cudaGraphExecDestroy(g->exec);
-        if (g->graph) cudaGraphDestroy(g->graph);
-        g->exec = nullptr; g->graph = nullptr;
-    }
-    void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wall_nodes, h->links, h->link_part, h->block_part, h->block_part_b,
-                    h->ordermap, h->chg_node, h->chg_key, h->cand, h->mark, h->traj, h->sq, h->scratch, h->small};
-    for (void* q : ptrs) if (q) cudaFree(q);
-    if (h->own) cudaStreamDestroy(h->own);
-    if (h->cap) cudaStreamDestroy(h->cap);
+void drop_graph(lbmgpu_handle* h) {
+    if (h->g.exec) cudaGraphExecDestroy(h->g.exec);
+    if (h->g.graph) cudaGraphDestroy(h->g.graph);
+    h->g = Graph{};
 }
 
-// ---- one time step ---------------------------------------------------------
-// fused = 1: the time-loop body of main.cpp:60-64; fused = 0: LBM::step only.
-void issue_step(lbmgpu_handle* h, cudaStream_t st, int par, bool macro, int fused) {
-    const StreamArgs a = stream_args(h, fused);
-    h->lz->stream(par, h->has_sq != 0, macro, h->L, a, h->geom, st);
-    int k = h->geom.bgrid ? 2 : 1;
-    if (macro) { k_finalize<<<1, 256, 0, st>>>(h->block_part_b, h->nblocks_b, h->sq); ++k; }
-    if (h->has_sq && fused) {
-        h->lz->squirmer(h->L, squirmer_args(h, par ^ 1, STAGE_FORCE | STAGE_BODY | STAGE_REMAP | STAGE_LOOP), st);
+void free_all(lbmgpu_handle* h) {
+    drop_graph(h);
+    void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wallrows, h->links, h->linkslot,
+                    h->link_part, h->block_part, h->block_part_b, h->ordermap, h->chg_node, h->chg_key,
+                    h->cand, h->mark, h->traj, h->sq, h->scratch, h->small};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    for (cudaEvent_t e : {h->ev_b[0], h->ev_b[1], h->ev_z, h->ev_s, h->ev_fork, h->ev_join})
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : {h->own, h->zs, h->cap, h->cap2})
+        if (s) cudaStreamDestroy(s);
+}
+
+StepPlan plan_step(lbmgpu_handle* h, long long s, bool macro, bool apply) {
+    StepPlan sp;
+    sp.s = s;
+    sp.par = (int)((s - 1) & 1);
+    sp.zslot = (int)(s % ZONE_SLOTS);
+    sp.corr = is_corr_step(h, s);
+    sp.apply = apply;
+    sp.macro = macro;
+    return sp;
+}
+
+// One time step of the time loop, B on stream a, Z and S on stream b (see the
+// dependency list at the top of this file). When called for step s, ev_b[s&1]
+// marks B(s-1)... precisely: ev_b[(s-1)&1] marks B(s-1), ev_z marks Z(s-1) and
+// ev_s marks S(s-1).
+void issue_fused(lbmgpu_handle* h, cudaStream_t sa, cudaStream_t sb, const StepPlan& sp) {
+    const StreamArgs a = stream_args(h, sp);
+    const int par = sp.par;
+    cudaStreamWaitEvent(sa, h->ev_z, 0);
+    if (sp.apply) cudaStreamWaitEvent(sa, h->ev_s, 0);
+    h->lz->bulk(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sa);
+    cudaEventRecord(h->ev_b[sp.s & 1], sa);
+    cudaStreamWaitEvent(sb, h->ev_b[(sp.s - 1) & 1], 0);
+    int k = 1;
+    if (h->geom.nwallrows) { h->lz->wallrows(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sb); ++k; }
+    if (h->geom.bgrid) { h->lz->zone(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sb); ++k; }
+    cudaEventRecord(h->ev_z, sb);
+    if (sp.macro) {
+        cudaStreamWaitEvent(sb, h->ev_b[sp.s & 1], 0);
+        k_finalize<<<1, 256, 0, sb>>>(h->block_part, h->nblocks, h->block_part_b, h->geom.bgrid ? h->nblocks_b : 0, h->sq);
+        ++k;
+    }
+    if (h->has_sq) {
+        if (sp.corr) cudaStreamWaitEvent(sb, h->ev_b[sp.s & 1], 0);
+        const int za = (int)((sp.s + 2) % ZONE_SLOTS);
+        h->lz->squirmer(h->L, squirmer_args(h, par ^ 1, STAGE_FORCE | STAGE_BODY | STAGE_REMAP | STAGE_LOOP,
+                                            sp.corr ? 1 : 0, za, -1), sb);
+        cudaEventRecord(h->ev_s, sb);
         ++k;
     }
     h->launches += k;
 }
 
-int ensure_graph(lbmgpu_handle* h, GraphSlot& g, int steps) {
-    if (g.exec) return LBMGPU_OK;
+// Make the events describe "everything issued so far on stream sa" before a
+// sequence of fused steps on (sa, sb), and join sb back into sa after it.
+void fused_begin(lbmgpu_handle* h, cudaStream_t sa, cudaStream_t sb) {
+    cudaEventRecord(h->ev_fork, sa);
+    cudaStreamWaitEvent(sb, h->ev_fork, 0);
+    for (cudaEvent_t e : {h->ev_b[0], h->ev_b[1], h->ev_z, h->ev_s}) cudaEventRecord(e, sa);
+}
+void fused_end(lbmgpu_handle* h, cudaStream_t sa, cudaStream_t sb) {
+    cudaEventRecord(h->ev_join, sb);
+    cudaStreamWaitEvent(sa, h->ev_join, 0);
+}
+
+int ensure_graph(lbmgpu_handle* h, int steps) {
+    if (h->g.exec && h->g.steps == steps) return LBMGPU_OK;
+    drop_graph(h);
     CUDA_TRY(h, cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
     const long long saved = h->launches;
-    for (int k = 0; k < steps; ++k) issue_step(h, h->cap, k & 1, false, 1);
+    fused_begin(h, h->cap, h->cap2);
+    // the pattern starts at a step s with (s - 1) % period == 0
+    for (int k = 0; k < steps; ++k) {
+        const long long s = 1 + k;
+        const bool apply = k > 0 && is_corr_step(h, s - 1);
+        issue_fused(h, h->cap, h->cap2, plan_step(h, s, false, apply));
+    }
+    fused_end(h, h->cap, h->cap2);
     h->launches = saved;
-    CUDA_TRY(h, cudaStreamEndCapture(h->cap, &g.graph));
-    CUDA_TRY(h, cudaGraphInstantiate(&g.exec, g.graph, 0));
+    CUDA_TRY(h, cudaStreamEndCapture(h->cap, &h->g.graph));
+    CUDA_TRY(h, cudaGraphInstantiate(&h->g.exec, h->g.graph, 0));
+    h->g.steps = steps;
     return LBMGPU_OK;
 }
 
@@ -448,8 +556,14 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     } while (0)
     CTRY(cudaSetDevice(p->device));
     CTRY(h->lz->prepare());
+    int prio_lo = 0, prio_hi = 0;
+    CTRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CTRY(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+    CTRY(cudaStreamCreateWithPriority(&h->zs, cudaStreamNonBlocking, prio_hi));
     CTRY(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+    CTRY(cudaStreamCreateWithPriority(&h->cap2, cudaStreamNonBlocking, prio_hi));
+    for (cudaEvent_t* e : {&h->ev_b[0], &h->ev_b[1], &h->ev_z, &h->ev_s, &h->ev_fork, &h->ev_join})
+        CTRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     h->stream = h->own;
 
     Lattice& L = h->L;
@@ -473,8 +587,8 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     const size_t N = L.N;
 
     HostInit hi;
-    build_initial(*p, L, hi);
-    h->n_wall = (int)hi.wall_nodes.size();
+    build_initial(*p, hi);
+    h->geom.nwallrows = (unsigned)(hi.wallrows.size() / 2);
     const int box = h->has_sq ? 2 * (int)std::ceil(p->radius) + 8 : 1;
     const long long boxvol = (long long)box * box * box;
     h->link_cap = (int)std::max<long long>(boxvol, (long long)hi.links.size() + 1);
@@ -484,9 +598,20 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
         h->geom.block = dim3(tx, 1, 1);
         h->geom.grid = dim3((p->nx + tx - 1) / tx, p->ny, p->nz);
         h->nblocks = h->geom.grid.x * h->geom.grid.y * h->geom.grid.z;
-        const long long nb = (long long)h->n_wall + (h->has_sq ? h->link_cap : 0);
+        if (h->has_sq) {
+            h->zw[0] = zone_width(p->radius, p->nx, false);
+            h->zw[1] = zone_width(p->radius, p->ny, p->walls_y != 0);
+            h->zw[2] = zone_width(p->radius, p->nz, p->walls_z != 0);
+            h->zone_cells = h->zw[0] * h->zw[1] * h->zw[2];
+        }
+        const long long nb = (long long)h->zone_cells;
         h->geom.bgrid = (unsigned)((nb + BOUNDARY_BLOCK - 1) / BOUNDARY_BLOCK);
         h->nblocks_b = std::max(1u, h->geom.bgrid);
+        // period of the launch pattern: AA parity (2), zone slots (3), mass correction (k)
+        const int k = p->mass_correction_every;
+        const int base = std::lcm(2, ZONE_SLOTS);
+        h->corr_in_graph = h->has_sq && k > 0 && std::lcm(base, k) <= MAX_PERIOD;
+        h->period = h->corr_in_graph ? std::lcm(base, k) : base;
     }
 
     CTRY(cudaMalloc(&h->f, (size_t)Q * N * h->esize));
@@ -498,12 +623,13 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     CTRY(cudaMalloc(&h->scratch, N * sizeof(double)));
     CTRY(cudaMalloc(&h->block_part, (size_t)h->nblocks * BLOCK_PART * sizeof(double)));
     CTRY(cudaMalloc(&h->block_part_b, (size_t)h->nblocks_b * BLOCK_PART * sizeof(double)));
-    CTRY(cudaMalloc(&h->wall_nodes, std::max<size_t>(1, hi.wall_nodes.size()) * sizeof(int)));
+    CTRY(cudaMalloc(&h->wallrows, std::max<size_t>(2, hi.wallrows.size()) * sizeof(int)));
     CTRY(cudaMalloc(&h->sq, sizeof(SqState)));
     CTRY(cudaMalloc(&h->small, (2 * MASS_GRID + 4 * DIAG_GRID + 16) * sizeof(double)));
     CTRY(cudaMalloc(&h->links, (size_t)h->link_cap * sizeof(int)));
     CTRY(cudaMalloc(&h->link_part, (size_t)h->link_cap * LINK_PART * sizeof(double)));
     if (h->has_sq) {
+        CTRY(cudaMalloc(&h->linkslot, N * sizeof(int)));
         CTRY(cudaMalloc(&h->ordermap, N * sizeof(int)));
         CTRY(cudaMalloc(&h->chg_node, (size_t)h->chg_cap * sizeof(int)));
         CTRY(cudaMalloc(&h->chg_key, (size_t)h->chg_cap * sizeof(int)));
@@ -517,24 +643,27 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     k_fill_d<<<592, 256, 0, st>>>(h->ux, N, 0.0);
     k_fill_d<<<592, 256, 0, st>>>(h->uy, N, 0.0);
     k_fill_d<<<592, 256, 0, st>>>(h->uz, N, 0.0);
+    h->launches += 5;
     CTRY(cudaMemsetAsync(h->block_part, 0, (size_t)h->nblocks * BLOCK_PART * sizeof(double), st));
     CTRY(cudaMemsetAsync(h->block_part_b, 0, (size_t)h->nblocks_b * BLOCK_PART * sizeof(double), st));
-    if (!hi.wall_nodes.empty())
-        CTRY(cudaMemcpyAsync(h->wall_nodes, hi.wall_nodes.data(), hi.wall_nodes.size() * sizeof(int),
+    if (!hi.wallrows.empty())
+        CTRY(cudaMemcpyAsync(h->wallrows, hi.wallrows.data(), hi.wallrows.size() * sizeof(int),
                              cudaMemcpyHostToDevice, st));
     CTRY(cudaMemsetAsync(h->link_part, 0, (size_t)h->link_cap * LINK_PART * sizeof(double), st));
     CTRY(cudaMemcpyAsync(h->flag, hi.flag.data(), N, cudaMemcpyHostToDevice, st));
     if (h->has_sq) {
         k_fill_i<<<592, 256, 0, st>>>(h->ordermap, N, -1);
-        if (!hi.links.empty())
+        CTRY(cudaMemsetAsync(h->linkslot, 0, N * sizeof(int), st));
+        if (!hi.links.empty()) {
             CTRY(cudaMemcpyAsync(h->links, hi.links.data(), hi.links.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            k_scatter_slots<<<64, 256, 0, st>>>(h->links, (int)hi.links.size(), h->linkslot);
+        }
+        h->launches += 2;
         CTRY(cudaMemsetAsync(h->traj, 0, (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double), st));
     }
-    CTRY(cudaStreamSynchronize(st));  // host vectors go out of scope
     CTRY(cudaMemcpyAsync(h->sq, &hi.s, sizeof(SqState), cudaMemcpyHostToDevice, st));
-    CTRY(cudaStreamSynchronize(st));
+    CTRY(cudaStreamSynchronize(st));  // host vectors go out of scope
     CTRY(cudaGetLastError());
-    h->launches += 5 + (h->has_sq ? 1 : 0);
 #undef CTRY
     *out = h;
     return LBMGPU_OK;
@@ -544,6 +673,7 @@ int lbmgpu_destroy(lbmgpu_handle* h) {
     if (!h) return LBMGPU_OK;
     cudaSetDevice(h->p.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->zs) cudaStreamSynchronize(h->zs);
     free_all(h);
     delete h;
     return LBMGPU_OK;
@@ -554,44 +684,64 @@ int lbmgpu_run(lbmgpu_handle* h, int nsteps) {
     if (nsteps < 0) return fail(h, LBMGPU_ERR_INVALID, "nsteps must be >= 0");
     if (nsteps == 0) return LBMGPU_OK;
     CUDA_TRY(h, cudaSetDevice(h->p.device));
-    const int per_step = (h->geom.bgrid ? 2 : 1) + (h->has_sq ? 1 : 0);
-    int rem = nsteps;
-    while (rem > 1) {
-        if (h->t_main & 1) {
-            issue_step(h, h->stream, 1, false, 1);
-            ++h->t_main; --rem;
-        } else if (rem - 1 >= GRAPH_LONG) {
-            int rc = ensure_graph(h, h->g_long, GRAPH_LONG);
-            if (rc) return rc;
-            CUDA_TRY(h, cudaGraphLaunch(h->g_long.exec, h->stream));
-            h->launches += (long long)GRAPH_LONG * per_step;
-            h->t_main += GRAPH_LONG; rem -= GRAPH_LONG;
-        } else if (rem - 1 >= 2) {
-            int rc = ensure_graph(h, h->g_short, 2);
-            if (rc) return rc;
-            CUDA_TRY(h, cudaGraphLaunch(h->g_short.exec, h->stream));
-            h->launches += 2 * per_step;
-            h->t_main += 2; rem -= 2;
-        } else {
-            issue_step(h, h->stream, (int)(h->t_main & 1), false, 1);
-            ++h->t_main; --rem;
+    cudaStream_t sa = h->stream, sb = h->zs;
+    const int per_step = 1 + (h->geom.nwallrows ? 1 : 0) + (h->geom.bgrid ? 1 : 0) + (h->has_sq ? 1 : 0);
+    const int gsteps = h->period * ((MIN_GRAPH + h->period - 1) / h->period);
+    fused_begin(h, sa, sb);
+    long long rem = nsteps;
+    while (rem > 0) {
+        const long long s = h->t_main + 1;
+        const bool last = rem == 1;
+        // A captured graph starts at a pattern boundary, ends before the last
+        // step (which stores the macroscopic fields), and contains correction
+        // steps only if the pattern period includes them.
+        bool graph_ok = !last && h->t_main % h->period == 0 && rem - 1 >= gsteps && !h->pending_corr;
+        if (graph_ok && h->has_sq && h->p.mass_correction_every > 0 && !h->corr_in_graph) {
+            const int k = h->p.mass_correction_every;
+            graph_ok = (h->t_main / k) == ((h->t_main + gsteps) / k);  // no correction step inside
         }
+        if (graph_ok) {
+            // the graph carries its own fork and join on the caller's stream
+            fused_end(h, sa, sb);
+            int rc = ensure_graph(h, gsteps);
+            if (rc) return rc;
+            CUDA_TRY(h, cudaGraphLaunch(h->g.exec, sa));
+            h->launches += (long long)gsteps * per_step;
+            h->t_main += gsteps;
+            rem -= gsteps;
+            h->pending_corr = is_corr_step(h, h->t_main);
+            fused_begin(h, sa, sb);
+            continue;
+        }
+        issue_fused(h, sa, sb, plan_step(h, s, last, h->pending_corr));
+        h->t_main = s;
+        h->pending_corr = is_corr_step(h, s);
+        --rem;
     }
-    issue_step(h, h->stream, (int)(h->t_main & 1), true, 1);  // last step: macro fields + wall force
-    ++h->t_main;
+    fused_end(h, sa, sb);
     return check_status(h);
 }
 
+// LBM::step alone: both collide-stream kernels, then the sphere force of the
+// step (lbm.cpp:219-223), all on the caller's stream.
 int lbmgpu_step(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
     CUDA_TRY(h, cudaSetDevice(h->p.device));
-    issue_step(h, h->stream, (int)(h->t_main & 1), true, 0);
+    StepPlan sp = plan_step(h, h->t_main + 1, true, h->pending_corr);
+    sp.corr = false;
+    const StreamArgs a = stream_args(h, sp);
+    cudaStream_t st = h->stream;
+    h->lz->bulk(sp.par, h->has_sq != 0, true, h->L, a, h->geom, st);
+    if (h->geom.nwallrows) { h->lz->wallrows(sp.par, h->has_sq != 0, true, h->L, a, h->geom, st); ++h->launches; }
+    if (h->geom.bgrid) { h->lz->zone(sp.par, h->has_sq != 0, true, h->L, a, h->geom, st); ++h->launches; }
+    k_finalize<<<1, 256, 0, st>>>(h->block_part, h->nblocks, h->block_part_b, h->geom.bgrid ? h->nblocks_b : 0, h->sq);
+    h->launches += 2;
     if (h->has_sq) {
-        // the tail of LBM::step: Fh, Th of this step (lbm.cpp:220-223)
-        h->lz->squirmer(h->L, squirmer_args(h, (int)((h->t_main + 1) & 1), STAGE_FORCE), h->stream);
-        k_clear_pending<<<1, 32, 0, h->stream>>>(h->sq);
+        h->lz->squirmer(h->L, squirmer_args(h, sp.par ^ 1, STAGE_FORCE, 0, -1, -1), st);
+        k_clear_pending<<<1, 32, 0, st>>>(h->sq);
         h->launches += 2;
     }
+    h->pending_corr = false;
     ++h->t_main;
     return check_status(h);
 }
@@ -600,7 +750,9 @@ int lbmgpu_advance_squirmer(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
     if (!h->has_sq) return LBMGPU_OK;  // LBM::advanceSquirmer returns without a squirmer (lbm.cpp:258)
     CUDA_TRY(h, cudaSetDevice(h->p.device));
-    h->lz->squirmer(h->L, squirmer_args(h, (int)(h->t_main & 1), STAGE_BODY | STAGE_REMAP), h->stream);
+    const long long s = h->t_main;  // the step just done
+    h->lz->squirmer(h->L, squirmer_args(h, (int)(h->t_main & 1), STAGE_BODY | STAGE_REMAP, 0,
+                                        (int)((s + 1) % ZONE_SLOTS), (int)((s + 2) % ZONE_SLOTS)), h->stream);
     ++h->launches;
     return check_status(h);
 }
@@ -608,11 +760,12 @@ int lbmgpu_advance_squirmer(lbmgpu_handle* h) {
 int lbmgpu_correct_mass(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
     CUDA_TRY(h, cudaSetDevice(h->p.device));
-    // a correction still pending from lbmgpu_run is applied first
+    // a correction still pending from lbmgpu_run is folded in and applied now
     double* part = h->small;
     double* dflag = h->small + 2 * MASS_GRID;
     h->lz->correct_mass(h->L, h->f, h->flag, (int)(h->t_main & 1), h->sq, part, dflag, h->stream);
     h->launches += 3;
+    h->pending_corr = false;
     return check_status(h);
 }
 
@@ -647,14 +800,7 @@ int lbmgpu_set_squirmer_state(lbmgpu_handle* h, const double X[3], const double 
     CUDA_TRY(h, cudaMemcpyAsync(&s, h->sq, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     for (int d = 0; d < 3; ++d) { s.X[d] = X[d]; s.e[d] = e[d]; s.U[d] = U[d]; s.W[d] = W[d]; }
-    int lo[3], w[3];
-    h_box(h->p, s, lo, w);
-    const int nd[3] = {h->p.nx, h->p.ny, h->p.nz};
-    for (int d = 0; d < 3; ++d) {
-        const int ww = w[d] + 4;
-        s.rb_w[d] = std::min(ww, nd[d]);
-        s.rb_lo[d] = ww >= nd[d] ? 0 : (((lo[d] - 2) % nd[d]) + nd[d]) % nd[d];
-    }
+    set_zones(h->p, s);
     CUDA_TRY(h, cudaMemcpyAsync(h->sq, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return LBMGPU_OK;
@@ -665,9 +811,7 @@ int lbmgpu_fields(lbmgpu_handle* h, uint8_t* flag, double* rho, double* u3) {
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     const size_t N = h->L.N;
     cudaStream_t st = h->stream;
-    if (flag) {
-        CUDA_TRY(h, cudaMemcpyAsync(flag, h->flag, N, cudaMemcpyDeviceToHost, st));
-    }
+    if (flag) CUDA_TRY(h, cudaMemcpyAsync(flag, h->flag, N, cudaMemcpyDeviceToHost, st));
     if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, h->rho, N * sizeof(double), cudaMemcpyDeviceToHost, st));
     std::vector<double> tmp;
     if (u3) {
@@ -720,8 +864,8 @@ int lbmgpu_traj_rows(lbmgpu_handle* h, double* rows, int max_rows, int* nrows, l
     }
     const long long avail = cnt - first;
     const int take = (int)std::min<long long>(avail, max_rows);
-    std::vector<double> ring((size_t)TRAJ_RING * TRAJ_COLS);
     if (take > 0) {
+        std::vector<double> ring((size_t)TRAJ_RING * TRAJ_COLS);
         CUDA_TRY(h, cudaMemcpyAsync(ring.data(), h->traj, ring.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         for (int k = 0; k < take; ++k) {
@@ -761,6 +905,7 @@ int lbmgpu_set_populations(lbmgpu_handle* h, const double* f) {
     }
     k_clear_pending<<<1, 32, 0, h->stream>>>(h->sq);
     ++h->launches;
+    h->pending_corr = false;
     return check_status(h);
 }
 
@@ -769,6 +914,57 @@ int lbmgpu_set_stream(lbmgpu_handle* h, void* cuda_stream) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own;
     return LBMGPU_OK;
+}
+
+int lbmgpu_time_kernels(lbmgpu_handle* h, int reps, double ms[3]) {
+    if (!h || !ms || reps < 1) return LBMGPU_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->p.device));
+    reps += reps & 1;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(h, cudaEventCreate(&e0));
+    CUDA_TRY(h, cudaEventCreate(&e1));
+    cudaStream_t st = h->stream;
+    float t = 0.f;
+    auto plan = [&](int k) { return plan_step(h, h->t_main + 1 + k, false, false); };
+    // bulk kernel alone
+    CUDA_TRY(h, cudaEventRecord(e0, st));
+    for (int k = 0; k < reps; ++k) {
+        const StepPlan sp = plan(k);
+        h->lz->bulk(sp.par, h->has_sq != 0, false, h->L, stream_args(h, sp), h->geom, st);
+    }
+    CUDA_TRY(h, cudaEventRecord(e1, st));
+    CUDA_TRY(h, cudaEventSynchronize(e1));
+    CUDA_TRY(h, cudaEventElapsedTime(&t, e0, e1));
+    ms[0] = t / reps;
+    h->launches += reps;
+    // zone kernel alone
+    ms[1] = 0.0;
+    if (h->geom.bgrid) {
+        CUDA_TRY(h, cudaEventRecord(e0, st));
+        for (int k = 0; k < reps; ++k) {
+            const StepPlan sp = plan(k);
+            h->lz->zone(sp.par, h->has_sq != 0, false, h->L, stream_args(h, sp), h->geom, st);
+        }
+        CUDA_TRY(h, cudaEventRecord(e1, st));
+        CUDA_TRY(h, cudaEventSynchronize(e1));
+        CUDA_TRY(h, cudaEventElapsedTime(&t, e0, e1));
+        ms[1] = t / reps;
+        h->launches += reps;
+    }
+    ms[2] = 0.0;
+    if (h->has_sq) {
+        CUDA_TRY(h, cudaEventRecord(e0, st));
+        for (int k = 0; k < reps; ++k)
+            h->lz->squirmer(h->L, squirmer_args(h, (int)(h->t_main & 1), STAGE_FORCE | STAGE_BODY | STAGE_REMAP, 0, -1, -1), st);
+        CUDA_TRY(h, cudaEventRecord(e1, st));
+        CUDA_TRY(h, cudaEventSynchronize(e1));
+        CUDA_TRY(h, cudaEventElapsedTime(&t, e0, e1));
+        ms[2] = t / reps;
+        h->launches += reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return check_status(h);
 }
 
 int lbmgpu_launch_count(const lbmgpu_handle* h, long long* n) {

@@ -57,6 +57,14 @@ class Solver:
         check(self.lib.lbmgpu_launch_count(self.h, ctypes.byref(v)), self.h)
         return v.value
 
+    def time_kernels(self, reps: int = 20) -> dict:
+        """Per-launch milliseconds of the bulk, zone and squirmer kernels,
+        each timed alone with CUDA events (advances the populations without
+        the sphere update: use on a handle kept for measurement)."""
+        ms = np.zeros(3)
+        check(self.lib.lbmgpu_time_kernels(self.h, int(reps), dptr(ms)), self.h)
+        return dict(bulk=ms[0], zone=ms[1], squirmer=ms[2])
+
     def set_stream(self, stream_handle: int | None) -> None:
         check(self.lib.lbmgpu_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), self.h)
 
