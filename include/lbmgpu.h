@@ -181,6 +181,64 @@ const char* lbmgpu_last_error(const lbmgpu_handle* h);
 
 int lbmgpu_abi_version(void);
 
+/* ---------------------------------------------------------------------------
+ * Ensembles (no counterpart in the reference, whose executable runs one
+ * lattice per process; parameter studies there launch the binary once per
+ * case, e.g. postprocessing/lbm_post.py:39-56 driving src/main.cpp).
+ *
+ * An ensemble advances n independent lattices ("members") together: one
+ * persistent bulk launch per step covers the rows of every member, one launch
+ * the zones around all squirmers and one the squirmer updates (a CTA per
+ * member), captured in CUDA graphs. Each member follows exactly the same
+ * arithmetic as a lattice created alone with lbmgpu_create, so its results
+ * are those of lbmgpu_run on that lattice.
+ * Members may differ in size (nx, ny, nz), squirmer geometry, swimming
+ * parameters, initial orientation and output cadence; they must share tau,
+ * lambda, the body force, the walls, precision, mass_correction_every,
+ * squirmer (on/off) and device.
+ * ------------------------------------------------------------------------- */
+typedef struct lbmgpu_batch lbmgpu_batch;
+
+/* Creates the n members from ps[0..n-1]. On failure *out is NULL and the
+ * message is available from lbmgpu_batch_last_error(NULL). */
+int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out);
+int lbmgpu_batch_destroy(lbmgpu_batch* b);
+
+/* nsteps time steps of every member (the loop body of lbmgpu_run). */
+int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps);
+
+/* The handle of member i, for the read-only calls: lbmgpu_time,
+ * lbmgpu_squirmer_state, lbmgpu_fields, lbmgpu_diag, lbmgpu_traj_rows,
+ * lbmgpu_get_populations, lbmgpu_launch_count, lbmgpu_last_error. Calls that
+ * advance or modify a member on its own return LBMGPU_ERR_INVALID. The handle
+ * is owned by the ensemble (do not destroy it). */
+int lbmgpu_batch_member(lbmgpu_batch* b, int i, lbmgpu_handle** h);
+
+/* Number of members and total lattice nodes (either pointer may be NULL). */
+int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
+
+/* Tiling of the bulk launch: threads_per_row (32, 64 or 128 threads cover
+ * one x-row) and ctas_per_sm (1..16; the grid is that many CTAs per SM). */
+int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int threads_per_row, int ctas_per_sm);
+
+/* Times the bulk launch for every tiling candidate, `reps` pairs of launches
+ * each, and keeps the fastest. The populations are saved to a temporary
+ * device buffer before and restored after, so the ensemble's state is
+ * unchanged. Outputs (may be NULL): the chosen tiling and its time per launch. */
+int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* ctas_per_sm, double* best_ms);
+
+/* Measurement aid: average device time of one bulk launch over all members
+ * with the current tiling (2*reps launches; the populations advance without
+ * the sphere update, as in lbmgpu_time_kernels). */
+int lbmgpu_batch_time_bulk(lbmgpu_batch* b, int reps, double* ms_per_launch);
+
+/* Runs the ensemble's caller-facing work on this cudaStream_t (NULL: the
+ * ensemble's own stream). The stream stays the caller's: it is not destroyed
+ * with the ensemble. */
+int lbmgpu_batch_set_stream(lbmgpu_batch* b, void* cuda_stream);
+int lbmgpu_batch_launch_count(const lbmgpu_batch* b, long long* n);
+const char* lbmgpu_batch_last_error(const lbmgpu_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

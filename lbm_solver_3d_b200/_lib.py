@@ -77,6 +77,17 @@ SIGNATURES = {
     "lbmgpu_time_kernels": (_I, [_P, _I, _DP]),
     "lbmgpu_last_error": (ctypes.c_char_p, [_P]),
     "lbmgpu_abi_version": (_I, []),
+    "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
+    "lbmgpu_batch_destroy": (_I, [_P]),
+    "lbmgpu_batch_run": (_I, [_P, _I]),
+    "lbmgpu_batch_member": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "lbmgpu_batch_size": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong)]),
+    "lbmgpu_batch_set_tiling": (_I, [_P, _I, _I]),
+    "lbmgpu_batch_autotune": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), _DP]),
+    "lbmgpu_batch_time_bulk": (_I, [_P, _I, _DP]),
+    "lbmgpu_batch_set_stream": (_I, [_P, _P]),
+    "lbmgpu_batch_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "lbmgpu_batch_last_error": (ctypes.c_char_p, [_P]),
 }
 
 _lib = None
@@ -109,6 +120,12 @@ def load():
 def check(code: int, handle=None) -> None:
     if code != LBMGPU_OK:
         msg = load().lbmgpu_last_error(handle)
+        raise LbmgpuError(code, msg.decode() if msg else "")
+
+
+def check_batch(code: int, batch=None) -> None:
+    if code != LBMGPU_OK:
+        msg = load().lbmgpu_batch_last_error(batch)
         raise LbmgpuError(code, msg.decode() if msg else "")
 
 

@@ -590,9 +590,6 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
 
 // Ensemble: one CTA per member, each with its own lattice and arguments; the
 // per-step settings are the same for all members.
-struct SqStep {
-    int parity, stages, corr_step, zslot_a, zslot_b;
-};
 template <class S>
 __global__ void __launch_bounds__(SQ_THREADS) k_squirmer_batch(const Lattice* lat, const SqArgs* args, SqStep st) {
     __shared__ Lattice L;

@@ -397,14 +397,15 @@ __global__ void __launch_bounds__(256, S::shifted ? 4 : 2) k_bulk(const Lattice 
 //  the next remap reads it) and write one row of link_part per near-particle
 //  node; wall force and mass go to block partials.
 // ---------------------------------------------------------------------------
+// The body of one zone thread (cell k of the zone); returns the sums for the
+// block reduction.
 template <class S, int PAR, bool SQ, bool MACRO>
-__global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
-    const int k = blockIdx.x * BOUNDARY_BLOCK + threadIdx.x;
+__device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a, int k, NodeSums& sums) {
     bool active = false;
     unsigned n = 0;
     int x = 0, y = 0, z = 0;
-    const ZoneBox* zb = SQ ? &a.sq->zone[a.zslot] : nullptr;
     if (SQ && k < a.zone_cells) {
+        const ZoneBox* zb = &a.sq->zone[a.zslot];
         const int bx = k % a.zw[0], by = (k / a.zw[0]) % a.zw[1], bz = k / (a.zw[0] * a.zw[1]);
         x = zb->lo[0] + bx; if (x >= L.nx) x -= L.nx;
         y = zb->lo[1] + by; z = zb->lo[2] + bz;
@@ -415,7 +416,6 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const 
             active = (a.flag[n] & TYPE_MASK) == T_FLUID;
         }
     }
-    NodeSums sums;
     if (active) {
         const uint8_t fl = a.flag[n];
         update_node<S, PAR, true, MACRO>(L, a, n, x, y, z, fl, 0, SQ || MACRO, sums);
@@ -425,6 +425,12 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const 
             lp[3] = sums.tp[0]; lp[4] = sums.tp[1]; lp[5] = sums.tp[2];
         }
     }
+}
+
+template <class S, int PAR, bool SQ, bool MACRO>
+__global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
+    NodeSums sums;
+    zone_cell<S, PAR, SQ, MACRO>(L, a, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums);
     if (MACRO || a.do_mass)
         block_reduce4<BOUNDARY_BLOCK>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass,
                                       a.block_part_b + (size_t)blockIdx.x * BLOCK_PART);

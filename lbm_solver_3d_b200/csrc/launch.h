@@ -20,6 +20,22 @@ struct StreamGeom {
     unsigned nwallrows;  // rows next to a wall (0: none)
 };
 
+struct SqArgs;
+
+// device tables of an ensemble
+struct BatchArgs {
+    const Lattice* lat;
+    const StreamArgs* args;
+    const SqArgs* sqargs;
+    const RowRef* rows;  int nrows;    // rows away from walls
+    const RowRef* wrows; int nwrows;   // rows next to a wall
+    double* row_part;                  // one entry per (member, y, z) row, both row kinds
+    double* zone_part;
+    int gzmax;                         // zone blocks per member (grid x of the zone launch)
+    int nmembers;
+    const MemberParts* parts;
+};
+
 struct Launchers {
     // the two collide-stream kernels of one time step
     void (*bulk)(int par, bool sq, bool macro, const Lattice& L, const StreamArgs& a, const StreamGeom& g,
@@ -38,6 +54,12 @@ struct Launchers {
     void (*correct_mass)(const Lattice& L, void* f, const uint8_t* flag, int P, SqState* sq, double* part,
                          double* dflag, cudaStream_t st);
     cudaError_t (*prepare)();  // one-time function attributes
+    // ensembles: the bulk rows (tx threads per row, grid CTAs), the zones,
+    // the squirmer updates and the wall forces of all members
+    void (*batch_bulk)(int par, bool macro, bool wallrows, int tx, int grid, const BatchArgs& b, BatchStep st,
+                       cudaStream_t s);
+    void (*batch_zone)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    void (*batch_squirmer)(const BatchArgs& b, SqStep st, cudaStream_t s);
 };
 
 const Launchers& launchers_f64();

@@ -176,4 +176,21 @@ struct StreamArgs {
     int apply_corr;               // add the pending correction on load (after one)
 };
 
+// ---- ensembles (k_batch.cuh) -------------------------------------------------
+constexpr int BATCH_MAX_NX = 256;   // longest x-row of an ensemble member
+
+struct RowRef {
+    int m, y, z;       // member, row coordinates
+    int part;          // entry of the row's partial sums (member base + y + ny*z)
+};
+struct BatchStep {     // per-step settings shared by all members
+    int zslot, do_mass, apply_corr;
+};
+struct SqStep {        // per-step settings of the members' squirmer updates
+    int parity, stages, corr_step, zslot_a, zslot_b;
+};
+struct MemberParts {   // where a member's partial sums live
+    int row0, nrow, nzb;  // ny*nz row entries from row0 (wall layers stay 0), zone blocks
+};
+
 }  // namespace lbmgpu

@@ -4,6 +4,7 @@
 // ============================================================================
 #pragma once
 #include "k_aux.cuh"
+#include "k_batch.cuh"
 #include "k_squirmer.cuh"
 #include "k_stream.cuh"
 #include "launch.h"
@@ -74,9 +75,55 @@ static void correct_mass_launch(const Lattice& L, void* f, const uint8_t* flag, 
     k_mass_apply<S><<<1184, AUX_BLOCK, 0, st>>>(L, f, flag, P, sq, dflag);
 }
 
+template <class S, int PAR, bool MACRO, bool WR>
+static void batch_bulk_tx(int tx, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    const RowRef* rows = WR ? b.wrows : b.rows;
+    const int n = WR ? b.nwrows : b.nrows;
+    double* part = b.row_part;
+    if (n == 0) return;
+    switch (tx) {
+        case 32: k_bulk_batch<S, PAR, MACRO, WR, 32><<<grid, 256, 0, s>>>(b.lat, b.args, rows, n, part, st); break;
+        case 64: k_bulk_batch<S, PAR, MACRO, WR, 64><<<grid, 256, 0, s>>>(b.lat, b.args, rows, n, part, st); break;
+        default: k_bulk_batch<S, PAR, MACRO, WR, 128><<<grid, 256, 0, s>>>(b.lat, b.args, rows, n, part, st); break;
+    }
+}
+
+template <class S>
+static void batch_bulk_launch(int par, bool macro, bool wr, int tx, int grid, const BatchArgs& b, BatchStep st,
+                              cudaStream_t s) {
+    switch ((par ? 4 : 0) | (macro ? 2 : 0) | (wr ? 1 : 0)) {
+        case 0: batch_bulk_tx<S, 0, false, false>(tx, grid, b, st, s); break;
+        case 1: batch_bulk_tx<S, 0, false, true>(tx, grid, b, st, s); break;
+        case 2: batch_bulk_tx<S, 0, true, false>(tx, grid, b, st, s); break;
+        case 3: batch_bulk_tx<S, 0, true, true>(tx, grid, b, st, s); break;
+        case 4: batch_bulk_tx<S, 1, false, false>(tx, grid, b, st, s); break;
+        case 5: batch_bulk_tx<S, 1, false, true>(tx, grid, b, st, s); break;
+        case 6: batch_bulk_tx<S, 1, true, false>(tx, grid, b, st, s); break;
+        default: batch_bulk_tx<S, 1, true, true>(tx, grid, b, st, s); break;
+    }
+}
+
+template <class S>
+static void batch_zone_launch(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    const dim3 grid(b.gzmax, b.nmembers);
+    switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
+        case 0: k_zone_batch<S, 0, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
+        case 1: k_zone_batch<S, 0, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
+        case 2: k_zone_batch<S, 1, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
+        default: k_zone_batch<S, 1, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
+    }
+}
+
+template <class S>
+static void batch_squirmer_launch(const BatchArgs& b, SqStep st, cudaStream_t s) {
+    k_squirmer_batch<S><<<b.nmembers, SQ_THREADS, squirmer_smem(), s>>>(b.lat, b.sqargs, st);
+}
+
 template <class S>
 static cudaError_t prepare_launch() {
-    return cudaFuncSetAttribute(k_squirmer<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+    cudaError_t e = cudaFuncSetAttribute(k_squirmer<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
 }
 
 template <class S>
@@ -91,6 +138,9 @@ static Launchers make_launchers() {
     l.set_pop = &set_pop_launch<S>;
     l.correct_mass = &correct_mass_launch<S>;
     l.prepare = &prepare_launch<S>;
+    l.batch_bulk = &batch_bulk_launch<S>;
+    l.batch_zone = &batch_zone_launch<S>;
+    l.batch_squirmer = &batch_squirmer_launch<S>;
     return l;
 }
 

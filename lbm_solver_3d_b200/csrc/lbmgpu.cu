@@ -98,6 +98,9 @@ struct lbmgpu_handle {
     bool pending_corr = false;   // a correction computed by the last step is still to be applied
     Graph g;
     std::string err;
+    // ensemble member: populations and flags live in the ensemble's pools,
+    // work is issued by the ensemble on its streams
+    bool member = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -400,6 +403,7 @@ void drop_graph(lbmgpu_handle* h) {
 
 void free_all(lbmgpu_handle* h) {
     drop_graph(h);
+    if (h->member) { h->f = nullptr; h->flag = nullptr; }
     void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wallrows, h->links, h->linkslot,
                     h->link_part, h->block_part, h->block_part_b, h->ordermap, h->chg_node, h->chg_key,
                     h->cand, h->mark, h->traj, h->sq, h->scratch, h->small};
@@ -472,10 +476,13 @@ int ensure_graph(lbmgpu_handle* h, int steps) {
     const long long saved = h->launches;
     fused_begin(h, h->cap, h->cap2);
     // the pattern starts at a step s with (s - 1) % period == 0
+    // (without corrections in the pattern, the graph is only launched over
+    // stretches that contain no correction step)
     for (int k = 0; k < steps; ++k) {
         const long long s = 1 + k;
-        const bool apply = k > 0 && is_corr_step(h, s - 1);
-        issue_fused(h, h->cap, h->cap2, plan_step(h, s, false, apply));
+        StepPlan sp = plan_step(h, s, false, h->corr_in_graph && k > 0 && is_corr_step(h, s - 1));
+        if (!h->corr_in_graph) sp.corr = false;
+        issue_fused(h, h->cap, h->cap2, sp);
     }
     fused_end(h, h->cap, h->cap2);
     h->launches = saved;
@@ -530,13 +537,25 @@ int lbmgpu_validate(const lbmgpu_params* p, char* msg, size_t msg_len) {
     return rc;
 }
 
-int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
+}  // extern "C"
+
+namespace {
+// Ensemble members: no streams of their own, populations and flags carved
+// from the ensemble's pools.
+struct MemberOpts {
+    cudaStream_t stream;
+    void* f;
+    uint8_t* flag;
+};
+
+int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** out) {
     if (!out) return fail(nullptr, LBMGPU_ERR_INVALID, "null output pointer");
     *out = nullptr;
     std::string m;
     if (validate_impl(p, m) != LBMGPU_OK) return fail(nullptr, LBMGPU_ERR_INVALID, m);
     lbmgpu_handle* h = new lbmgpu_handle();
     h->p = *p;
+    h->member = mo != nullptr;
     h->lz = launchers_for(p->precision);
     h->esize = esize_for(p->precision);
     h->has_sq = p->squirmer;
@@ -556,15 +575,19 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     } while (0)
     CTRY(cudaSetDevice(p->device));
     CTRY(h->lz->prepare());
-    int prio_lo = 0, prio_hi = 0;
-    CTRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    CTRY(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
-    CTRY(cudaStreamCreateWithPriority(&h->zs, cudaStreamNonBlocking, prio_hi));
-    CTRY(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
-    CTRY(cudaStreamCreateWithPriority(&h->cap2, cudaStreamNonBlocking, prio_hi));
-    for (cudaEvent_t* e : {&h->ev_b[0], &h->ev_b[1], &h->ev_z, &h->ev_s, &h->ev_fork, &h->ev_join})
-        CTRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    h->stream = h->own;
+    if (mo) {
+        h->stream = mo->stream;
+    } else {
+        int prio_lo = 0, prio_hi = 0;
+        CTRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+        CTRY(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+        CTRY(cudaStreamCreateWithPriority(&h->zs, cudaStreamNonBlocking, prio_hi));
+        CTRY(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+        CTRY(cudaStreamCreateWithPriority(&h->cap2, cudaStreamNonBlocking, prio_hi));
+        for (cudaEvent_t* e : {&h->ev_b[0], &h->ev_b[1], &h->ev_z, &h->ev_s, &h->ev_fork, &h->ev_join})
+            CTRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        h->stream = h->own;
+    }
 
     Lattice& L = h->L;
     L.nx = p->nx; L.ny = p->ny; L.nz = p->nz;
@@ -614,8 +637,13 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
         h->period = h->corr_in_graph ? std::lcm(base, k) : base;
     }
 
-    CTRY(cudaMalloc(&h->f, (size_t)Q * N * h->esize));
-    CTRY(cudaMalloc(&h->flag, N));
+    if (mo) {
+        h->f = mo->f;
+        h->flag = mo->flag;
+    } else {
+        CTRY(cudaMalloc(&h->f, (size_t)Q * N * h->esize));
+        CTRY(cudaMalloc(&h->flag, N));
+    }
     CTRY(cudaMalloc(&h->rho, N * sizeof(double)));
     CTRY(cudaMalloc(&h->ux, N * sizeof(double)));
     CTRY(cudaMalloc(&h->uy, N * sizeof(double)));
@@ -668,9 +696,15 @@ int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) {
     *out = h;
     return LBMGPU_OK;
 }
+}  // namespace
+
+extern "C" {
+
+int lbmgpu_create(const lbmgpu_params* p, lbmgpu_handle** out) { return create_impl(p, nullptr, out); }
 
 int lbmgpu_destroy(lbmgpu_handle* h) {
     if (!h) return LBMGPU_OK;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: destroy the ensemble");
     cudaSetDevice(h->p.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->zs) cudaStreamSynchronize(h->zs);
@@ -681,6 +715,7 @@ int lbmgpu_destroy(lbmgpu_handle* h) {
 
 int lbmgpu_run(lbmgpu_handle* h, int nsteps) {
     if (!h) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     if (nsteps < 0) return fail(h, LBMGPU_ERR_INVALID, "nsteps must be >= 0");
     if (nsteps == 0) return LBMGPU_OK;
     CUDA_TRY(h, cudaSetDevice(h->p.device));
@@ -726,6 +761,7 @@ int lbmgpu_run(lbmgpu_handle* h, int nsteps) {
 // step (lbm.cpp:219-223), all on the caller's stream.
 int lbmgpu_step(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     StepPlan sp = plan_step(h, h->t_main + 1, true, h->pending_corr);
     sp.corr = false;
@@ -748,6 +784,7 @@ int lbmgpu_step(lbmgpu_handle* h) {
 
 int lbmgpu_advance_squirmer(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     if (!h->has_sq) return LBMGPU_OK;  // LBM::advanceSquirmer returns without a squirmer (lbm.cpp:258)
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     const long long s = h->t_main;  // the step just done
@@ -759,6 +796,7 @@ int lbmgpu_advance_squirmer(lbmgpu_handle* h) {
 
 int lbmgpu_correct_mass(lbmgpu_handle* h) {
     if (!h) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     // a correction still pending from lbmgpu_run is folded in and applied now
     double* part = h->small;
@@ -794,6 +832,7 @@ int lbmgpu_squirmer_state(lbmgpu_handle* h, lbmgpu_squirmer* o) {
 int lbmgpu_set_squirmer_state(lbmgpu_handle* h, const double X[3], const double e[3], const double U[3],
                               const double W[3]) {
     if (!h || !X || !e || !U || !W) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     if (!h->has_sq) return fail(h, LBMGPU_ERR_INVALID, "no squirmer in this lattice");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     SqState s;
@@ -894,6 +933,7 @@ int lbmgpu_get_populations(lbmgpu_handle* h, double* f) {
 
 int lbmgpu_set_populations(lbmgpu_handle* h, const double* f) {
     if (!h || !f) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     const size_t N = h->L.N;
     const int P = (int)(h->t_main & 1);
@@ -911,6 +951,7 @@ int lbmgpu_set_populations(lbmgpu_handle* h, const double* f) {
 
 int lbmgpu_set_stream(lbmgpu_handle* h, void* cuda_stream) {
     if (!h) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own;
     return LBMGPU_OK;
@@ -918,6 +959,7 @@ int lbmgpu_set_stream(lbmgpu_handle* h, void* cuda_stream) {
 
 int lbmgpu_time_kernels(lbmgpu_handle* h, int reps, double ms[3]) {
     if (!h || !ms || reps < 1) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     reps += reps & 1;
     cudaEvent_t e0, e1;
@@ -976,6 +1018,520 @@ int lbmgpu_launch_count(const lbmgpu_handle* h, long long* n) {
 const char* lbmgpu_last_error(const lbmgpu_handle* h) {
     if (!h) return g_create_error.c_str();
     return h->err.c_str();
+}
+
+}  // extern "C"
+
+// ============================================================================
+//  Ensembles (lbmgpu_batch_*): many independent lattices advanced together
+//  by the batch kernels of k_batch.cuh.
+// ============================================================================
+namespace {
+
+// Wall force of every member on a macro step (one CTA per member): its row
+// entries, then its zone blocks, in the order and with the thread count of
+// k_finalize, so the result equals that of the lattice run alone.
+__global__ void k_finalize_batch(const MemberParts* __restrict__ mp, const double* row_part, const double* zone_part,
+                                 int gzmax, const StreamArgs* __restrict__ args) {
+    __shared__ double red[8][3];
+    const int m = blockIdx.x;
+    const MemberParts q = mp[m];
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int k = threadIdx.x; k < q.nrow + q.nzb; k += blockDim.x) {
+        const double* p = k < q.nrow ? row_part + (size_t)(q.row0 + k) * BLOCK_PART
+                                     : zone_part + ((size_t)m * gzmax + (k - q.nrow)) * BLOCK_PART;
+        a0 += p[0]; a1 += p[1]; a2 += p[2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_down_sync(0xffffffffu, a0, o);
+        a1 += __shfl_down_sync(0xffffffffu, a1, o);
+        a2 += __shfl_down_sync(0xffffffffu, a2, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5][0] = a0; red[threadIdx.x >> 5][1] = a1; red[threadIdx.x >> 5][2] = a2; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { s0 += red[w][0]; s1 += red[w][1]; s2 += red[w][2]; }
+        SqState* sq = args[m].sq;
+        sq->wall_force[0] = s0; sq->wall_force[1] = s1; sq->wall_force[2] = s2;
+    }
+}
+
+// status words of all members, OR-ed
+__global__ void k_batch_status(const StreamArgs* args, int n, int* out) {
+    int st = 0;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) st |= args[m].sq->status;
+    for (int o = 16; o > 0; o >>= 1) st |= __shfl_down_sync(0xffffffffu, st, o);
+    __shared__ int red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = st;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t |= red[w];
+        *out = t;
+    }
+}
+
+}  // namespace
+
+struct lbmgpu_batch {
+    std::vector<lbmgpu_handle*> m;
+    lbmgpu_params p0{};
+    const Launchers* lz = nullptr;
+    int has_sq = 0, period = 6, sms = 148;
+    bool corr_in_graph = false;
+    cudaStream_t own = nullptr;    // the ensemble's own caller-facing stream
+    cudaStream_t sa = nullptr;     // the caller-facing stream in use (own or the caller's)
+    cudaStream_t sb = nullptr, cap = nullptr, cap2 = nullptr;
+    cudaEvent_t ev_b[2] = {nullptr, nullptr}, ev_z = nullptr, ev_s = nullptr, ev_fork = nullptr, ev_join = nullptr;
+    void* fpool = nullptr;
+    uint8_t* flagpool = nullptr;
+    Lattice* d_lat = nullptr;
+    StreamArgs* d_args = nullptr;
+    SqArgs* d_sqargs = nullptr;
+    RowRef* d_rows = nullptr;
+    RowRef* d_wrows = nullptr;
+    MemberParts* d_parts = nullptr;
+    double *row_part = nullptr, *zone_part = nullptr;
+    int* d_status = nullptr;
+    BatchArgs ba{};
+    int tx = 32, bps = 4;          // tiling of the bulk launch (autotuned)
+    long long cells = 0, t = 0, launches = 0;
+    bool pending_corr = false;
+    Graph g;
+    std::string err;
+};
+
+namespace {
+
+int bfail(lbmgpu_batch* b, int code, const std::string& msg) {
+    if (b) b->err = msg; else g_create_error = msg;
+    return code;
+}
+
+#define BTRY(b, call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return bfail(b, e_ == cudaErrorMemoryAllocation ? LBMGPU_ERR_NOMEM : LBMGPU_ERR_CUDA,   \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+void batch_free(lbmgpu_batch* b) {
+    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
+    if (b->g.graph) cudaGraphDestroy(b->g.graph);
+    for (lbmgpu_handle* h : b->m) {
+        h->member = true;
+        free_all(h);
+        delete h;
+    }
+    b->m.clear();
+    void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts,
+                    b->row_part, b->zone_part, b->d_status};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    for (cudaEvent_t e : {b->ev_b[0], b->ev_b[1], b->ev_z, b->ev_s, b->ev_fork, b->ev_join})
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : {b->own, b->sb, b->cap, b->cap2})
+        if (s) cudaStreamDestroy(s);
+}
+
+bool is_corr_batch(const lbmgpu_batch* b, long long s) {
+    const int k = b->p0.mass_correction_every;
+    return b->has_sq && k > 0 && s % k == 0;
+}
+
+void issue_batch(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb, long long s, bool macro, bool apply,
+                 bool capture = false) {
+    const int par = (int)((s - 1) & 1);
+    const bool corr = is_corr_batch(b, s) && (!capture || b->corr_in_graph);
+    const BatchStep bst{(int)(s % ZONE_SLOTS), corr ? 1 : 0, apply ? 1 : 0};
+    const int grid = b->sms * b->bps;
+    cudaStreamWaitEvent(sa, b->ev_z, 0);
+    if (apply) cudaStreamWaitEvent(sa, b->ev_s, 0);
+    b->lz->batch_bulk(par, macro, false, b->tx, grid, b->ba, bst, sa);
+    cudaEventRecord(b->ev_b[s & 1], sa);
+    cudaStreamWaitEvent(sb, b->ev_b[(s - 1) & 1], 0);
+    int k = 1;
+    if (b->ba.nwrows) {
+        const int wgrid = std::max(1, std::min(grid, (b->ba.nwrows + 7) / 8));
+        b->lz->batch_bulk(par, macro, true, 32, wgrid, b->ba, bst, sb);
+        ++k;
+    }
+    if (b->has_sq) { b->lz->batch_zone(par, macro, b->ba, bst, sb); ++k; }
+    cudaEventRecord(b->ev_z, sb);
+    if (macro) {
+        cudaStreamWaitEvent(sb, b->ev_b[s & 1], 0);
+        k_finalize_batch<<<(unsigned)b->m.size(), 256, 0, sb>>>(b->d_parts, b->row_part, b->zone_part, b->ba.gzmax,
+                                                               b->d_args);
+        ++k;
+    }
+    if (b->has_sq) {
+        if (corr) cudaStreamWaitEvent(sb, b->ev_b[s & 1], 0);
+        const SqStep sst{par ^ 1, STAGE_FORCE | STAGE_BODY | STAGE_REMAP | STAGE_LOOP, corr ? 1 : 0,
+                         (int)((s + 2) % ZONE_SLOTS), -1};
+        b->lz->batch_squirmer(b->ba, sst, sb);
+        cudaEventRecord(b->ev_s, sb);
+        ++k;
+    }
+    b->launches += k;
+}
+
+void batch_begin(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb) {
+    cudaEventRecord(b->ev_fork, sa);
+    cudaStreamWaitEvent(sb, b->ev_fork, 0);
+    for (cudaEvent_t e : {b->ev_b[0], b->ev_b[1], b->ev_z, b->ev_s}) cudaEventRecord(e, sa);
+}
+void batch_end(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb) {
+    cudaEventRecord(b->ev_join, sb);
+    cudaStreamWaitEvent(sa, b->ev_join, 0);
+}
+
+int batch_graph(lbmgpu_batch* b, int steps) {
+    if (b->g.exec && b->g.steps == steps) return LBMGPU_OK;
+    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
+    if (b->g.graph) cudaGraphDestroy(b->g.graph);
+    b->g = Graph{};
+    BTRY(b, cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const long long saved = b->launches;
+    batch_begin(b, b->cap, b->cap2);
+    for (int k = 0; k < steps; ++k) {
+        const long long s = 1 + k;
+        issue_batch(b, b->cap, b->cap2, s, false, b->corr_in_graph && k > 0 && is_corr_batch(b, s - 1), true);
+    }
+    batch_end(b, b->cap, b->cap2);
+    b->launches = saved;
+    BTRY(b, cudaStreamEndCapture(b->cap, &b->g.graph));
+    BTRY(b, cudaGraphInstantiate(&b->g.exec, b->g.graph, 0));
+    b->g.steps = steps;
+    return LBMGPU_OK;
+}
+
+int batch_status(lbmgpu_batch* b) {
+    BTRY(b, cudaGetLastError());
+    k_batch_status<<<1, 256, 0, b->sa>>>(b->d_args, (int)b->m.size(), b->d_status);
+    int st = 0;
+    BTRY(b, cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->sa));
+    BTRY(b, cudaStreamSynchronize(b->sa));
+    if (st & ST_NAN) return bfail(b, LBMGPU_ERR_NAN, "non-finite squirmer force, torque or state in a member");
+    if (st & (ST_REMAP_RANGE | ST_LINK_OVERFLOW | ST_REMAP_OVERFLOW))
+        return bfail(b, LBMGPU_ERR_DEVICE, "a member's squirmer update failed a consistency check");
+    return LBMGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
+    if (!out || !ps || n < 1) return bfail(nullptr, LBMGPU_ERR_INVALID, "need at least one member");
+    *out = nullptr;
+    const lbmgpu_params& p0 = ps[0];
+    for (int i = 0; i < n; ++i) {
+        std::string m;
+        if (validate_impl(&ps[i], m) != LBMGPU_OK)
+            return bfail(nullptr, LBMGPU_ERR_INVALID, "member " + std::to_string(i) + ": " + m);
+        const lbmgpu_params& q = ps[i];
+        if (q.tau != p0.tau || q.lambda != p0.lambda || q.fx != p0.fx || q.fy != p0.fy || q.fz != p0.fz ||
+            q.walls_y != p0.walls_y || q.walls_z != p0.walls_z || q.precision != p0.precision ||
+            q.mass_correction_every != p0.mass_correction_every || q.squirmer != p0.squirmer || q.device != p0.device)
+            return bfail(nullptr, LBMGPU_ERR_INVALID,
+                         "member " + std::to_string(i) + ": members must share tau, lambda, body force, walls, "
+                         "precision, mass_correction_every, squirmer and device");
+        if (q.nx > BATCH_MAX_NX)
+            return bfail(nullptr, LBMGPU_ERR_INVALID,
+                         "member " + std::to_string(i) + ": nx must be <= " + std::to_string(BATCH_MAX_NX) + " in an ensemble");
+    }
+    lbmgpu_batch* b = new lbmgpu_batch();
+    b->p0 = p0;
+    b->lz = launchers_for(p0.precision);
+    b->has_sq = p0.squirmer;
+    auto bail = [&](int rc) {
+        g_create_error = b->err;
+        batch_free(b);
+        delete b;
+        return rc;
+    };
+#define CB(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            b->err = std::string(#call) + ": " + cudaGetErrorString(e_);                            \
+            return bail(e_ == cudaErrorMemoryAllocation ? LBMGPU_ERR_NOMEM : LBMGPU_ERR_CUDA);      \
+        }                                                                                           \
+    } while (0)
+    CB(cudaSetDevice(p0.device));
+    CB(b->lz->prepare());
+    CB(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, p0.device));
+    int prio_lo = 0, prio_hi = 0;
+    CB(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CB(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+    b->sa = b->own;
+    CB(cudaStreamCreateWithPriority(&b->sb, cudaStreamNonBlocking, prio_hi));
+    CB(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    CB(cudaStreamCreateWithPriority(&b->cap2, cudaStreamNonBlocking, prio_hi));
+    for (cudaEvent_t* e : {&b->ev_b[0], &b->ev_b[1], &b->ev_z, &b->ev_s, &b->ev_fork, &b->ev_join})
+        CB(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+
+    // the packed pools: every member's populations back to back, then flags
+    const size_t es = esize_for(p0.precision);
+    std::vector<size_t> foff(n), goff(n);
+    size_t ftot = 0, gtot = 0;
+    for (int i = 0; i < n; ++i) {
+        const size_t N = (size_t)ps[i].nx * ps[i].ny * ps[i].nz;
+        foff[i] = ftot; ftot += ((size_t)Q * N * es + 255) / 256 * 256;
+        goff[i] = gtot; gtot += (N + 255) / 256 * 256;
+        b->cells += (long long)N;
+    }
+    CB(cudaMalloc(&b->fpool, ftot));
+    CB(cudaMalloc(&b->flagpool, gtot));
+    for (int i = 0; i < n; ++i) {
+        MemberOpts mo{b->sa, static_cast<char*>(b->fpool) + foff[i], b->flagpool + goff[i]};
+        lbmgpu_handle* h = nullptr;
+        const int rc = create_impl(&ps[i], &mo, &h);
+        if (rc != LBMGPU_OK) {
+            b->err = "member " + std::to_string(i) + ": " + g_create_error;
+            return bail(rc);
+        }
+        b->m.push_back(h);
+    }
+
+    // rows (away from walls / next to a wall) and the partial-sum layout: each
+    // member owns ny*nz row entries indexed y + ny*z (the wall layers' stay 0)
+    // and gzmax zone-block entries, as a lattice run alone lays out its blocks
+    std::vector<RowRef> rows, wrows;
+    std::vector<MemberParts> parts(n);
+    int gzmax = 1;
+    size_t nparts = 0;
+    for (int i = 0; i < n; ++i) {
+        const lbmgpu_params& q = ps[i];
+        parts[i].row0 = (int)nparts;
+        parts[i].nrow = q.ny * q.nz;
+        for (int z = 0; z < q.nz; ++z)
+            for (int y = 0; y < q.ny; ++y) {
+                if (is_wall(q, y, z)) continue;
+                (near_wall(q, y, z) ? wrows : rows).push_back(RowRef{i, y, z, (int)nparts + y + q.ny * z});
+            }
+        nparts += (size_t)q.ny * q.nz;
+        parts[i].nzb = b->has_sq ? (int)b->m[i]->geom.bgrid : 0;
+        gzmax = std::max(gzmax, parts[i].nzb);
+    }
+    CB(cudaMalloc(&b->d_rows, std::max<size_t>(1, rows.size()) * sizeof(RowRef)));
+    CB(cudaMalloc(&b->d_wrows, std::max<size_t>(1, wrows.size()) * sizeof(RowRef)));
+    CB(cudaMalloc(&b->row_part, nparts * BLOCK_PART * sizeof(double)));
+    CB(cudaMalloc(&b->zone_part, (size_t)n * gzmax * BLOCK_PART * sizeof(double)));
+    CB(cudaMalloc(&b->d_parts, (size_t)n * sizeof(MemberParts)));
+    CB(cudaMalloc(&b->d_lat, (size_t)n * sizeof(Lattice)));
+    CB(cudaMalloc(&b->d_args, (size_t)n * sizeof(StreamArgs)));
+    CB(cudaMalloc(&b->d_sqargs, (size_t)n * sizeof(SqArgs)));
+    CB(cudaMalloc(&b->d_status, sizeof(int)));
+    std::vector<Lattice> lat(n);
+    std::vector<StreamArgs> args(n);
+    std::vector<SqArgs> sqa(n);
+    for (int i = 0; i < n; ++i) {
+        lbmgpu_handle* h = b->m[i];
+        lat[i] = h->L;
+        args[i] = stream_args(h, plan_step(h, 1, false, false));
+        sqa[i] = squirmer_args(h, 0, 0, 0, -1, -1);
+        sqa[i].block_part = b->row_part + (size_t)parts[i].row0 * BLOCK_PART;
+        sqa[i].nblocks = parts[i].nrow;
+        sqa[i].block_part_b = b->zone_part + (size_t)i * gzmax * BLOCK_PART;
+        sqa[i].nblocks_b = parts[i].nzb;
+        sqa[i].block_part_w = nullptr;
+        sqa[i].nblocks_w = 0;
+    }
+    cudaStream_t st = b->sa;
+    CB(cudaMemcpyAsync(b->d_rows, rows.data(), rows.size() * sizeof(RowRef), cudaMemcpyHostToDevice, st));
+    if (!wrows.empty())
+        CB(cudaMemcpyAsync(b->d_wrows, wrows.data(), wrows.size() * sizeof(RowRef), cudaMemcpyHostToDevice, st));
+    CB(cudaMemcpyAsync(b->d_parts, parts.data(), n * sizeof(MemberParts), cudaMemcpyHostToDevice, st));
+    CB(cudaMemcpyAsync(b->d_lat, lat.data(), n * sizeof(Lattice), cudaMemcpyHostToDevice, st));
+    CB(cudaMemcpyAsync(b->d_args, args.data(), n * sizeof(StreamArgs), cudaMemcpyHostToDevice, st));
+    CB(cudaMemcpyAsync(b->d_sqargs, sqa.data(), n * sizeof(SqArgs), cudaMemcpyHostToDevice, st));
+    CB(cudaMemsetAsync(b->row_part, 0, nparts * BLOCK_PART * sizeof(double), st));
+    CB(cudaMemsetAsync(b->zone_part, 0, (size_t)n * gzmax * BLOCK_PART * sizeof(double), st));
+    CB(cudaStreamSynchronize(st));
+    b->ba.lat = b->d_lat; b->ba.args = b->d_args; b->ba.sqargs = b->d_sqargs;
+    b->ba.rows = b->d_rows; b->ba.nrows = (int)rows.size();
+    b->ba.wrows = b->d_wrows; b->ba.nwrows = (int)wrows.size();
+    b->ba.row_part = b->row_part; b->ba.zone_part = b->zone_part;
+    b->ba.gzmax = gzmax; b->ba.nmembers = n; b->ba.parts = b->d_parts;
+    const int k = p0.mass_correction_every;
+    const int base = std::lcm(2, ZONE_SLOTS);
+    b->corr_in_graph = b->has_sq && k > 0 && std::lcm(base, k) <= MAX_PERIOD;
+    b->period = b->corr_in_graph ? std::lcm(base, k) : base;
+#undef CB
+    *out = b;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_destroy(lbmgpu_batch* b) {
+    if (!b) return LBMGPU_OK;
+    cudaSetDevice(b->p0.device);
+    if (b->sa) cudaStreamSynchronize(b->sa);
+    if (b->sb) cudaStreamSynchronize(b->sb);
+    batch_free(b);
+    delete b;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells) {
+    if (!b) return LBMGPU_ERR_INVALID;
+    if (members) *members = (int)b->m.size();
+    if (cells) *cells = b->cells;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_member(lbmgpu_batch* b, int i, lbmgpu_handle** h) {
+    if (!b || !h || i < 0 || i >= (int)b->m.size()) return bfail(b, LBMGPU_ERR_INVALID, "no such member");
+    *h = b->m[i];
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
+    if (!b) return LBMGPU_ERR_INVALID;
+    if (nsteps < 0) return bfail(b, LBMGPU_ERR_INVALID, "nsteps must be >= 0");
+    if (nsteps == 0) return LBMGPU_OK;
+    BTRY(b, cudaSetDevice(b->p0.device));
+    cudaStream_t sa = b->sa, sb = b->sb;
+    const int per_step = 1 + (b->ba.nwrows ? 1 : 0) + (b->has_sq ? 2 : 0);
+    const int gsteps = b->period * ((MIN_GRAPH + b->period - 1) / b->period);
+    batch_begin(b, sa, sb);
+    long long rem = nsteps;
+    while (rem > 0) {
+        const bool last = rem == 1;
+        bool graph_ok = !last && b->t % b->period == 0 && rem - 1 >= gsteps && !b->pending_corr;
+        if (graph_ok && b->has_sq && b->p0.mass_correction_every > 0 && !b->corr_in_graph) {
+            const int k = b->p0.mass_correction_every;
+            graph_ok = (b->t / k) == ((b->t + gsteps) / k);
+        }
+        if (graph_ok) {
+            batch_end(b, sa, sb);
+            int rc = batch_graph(b, gsteps);
+            if (rc) return rc;
+            BTRY(b, cudaGraphLaunch(b->g.exec, sa));
+            b->launches += (long long)gsteps * per_step;
+            b->t += gsteps;
+            rem -= gsteps;
+            b->pending_corr = is_corr_batch(b, b->t);
+            batch_begin(b, sa, sb);
+            continue;
+        }
+        const long long s = b->t + 1;
+        issue_batch(b, sa, sb, s, last, b->pending_corr);
+        b->t = s;
+        b->pending_corr = is_corr_batch(b, s);
+        --rem;
+    }
+    batch_end(b, sa, sb);
+    for (lbmgpu_handle* h : b->m) { h->t_main = b->t; h->pending_corr = b->pending_corr; }
+    return batch_status(b);
+}
+
+int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int threads_per_row, int ctas_per_sm) {
+    if (!b) return LBMGPU_ERR_INVALID;
+    if ((threads_per_row != 32 && threads_per_row != 64 && threads_per_row != 128) || ctas_per_sm < 1 || ctas_per_sm > 16)
+        return bfail(b, LBMGPU_ERR_INVALID, "threads_per_row must be 32, 64 or 128 and ctas_per_sm 1..16");
+    b->tx = threads_per_row;
+    b->bps = ctas_per_sm;
+    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
+    if (b->g.graph) cudaGraphDestroy(b->g.graph);
+    b->g = Graph{};
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* ctas_per_sm, double* best_ms) {
+    if (!b || reps < 1) return LBMGPU_ERR_INVALID;
+    BTRY(b, cudaSetDevice(b->p0.device));
+    cudaStream_t st = b->sa;
+    BTRY(b, cudaStreamSynchronize(b->sb));
+    // the candidates run real steps (without the sphere update); the
+    // populations are saved first and restored afterwards
+    size_t bytes = 0;
+    for (lbmgpu_handle* h : b->m) bytes += ((size_t)Q * h->L.N * h->esize + 255) / 256 * 256;
+    void* save = nullptr;
+    BTRY(b, cudaMalloc(&save, bytes));
+    BTRY(b, cudaMemcpyAsync(save, b->fpool, bytes, cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0, e1;
+    BTRY(b, cudaEventCreate(&e0));
+    BTRY(b, cudaEventCreate(&e1));
+    const int txs[3] = {32, 64, 128};
+    const int bpss[6] = {1, 2, 3, 4, 6, 8};
+    double best = 1e30;
+    int btx = b->tx, bbps = b->bps;
+    const BatchStep bst{(int)((b->t + 1) % ZONE_SLOTS), 0, 0};
+    for (int tx : txs)
+        for (int bps : bpss) {
+            const int grid = b->sms * bps;
+            b->lz->batch_bulk(0, false, false, tx, grid, b->ba, bst, st);  // warm-up
+            b->lz->batch_bulk(1, false, false, tx, grid, b->ba, bst, st);
+            BTRY(b, cudaEventRecord(e0, st));
+            for (int r = 0; r < reps; ++r) {
+                b->lz->batch_bulk(0, false, false, tx, grid, b->ba, bst, st);
+                b->lz->batch_bulk(1, false, false, tx, grid, b->ba, bst, st);
+            }
+            BTRY(b, cudaEventRecord(e1, st));
+            BTRY(b, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BTRY(b, cudaEventElapsedTime(&ms, e0, e1));
+            b->launches += 2 * reps + 2;
+            const double per = ms / (2.0 * reps);
+            if (per < best) { best = per; btx = tx; bbps = bps; }
+        }
+    BTRY(b, cudaMemcpyAsync(b->fpool, save, bytes, cudaMemcpyDeviceToDevice, st));
+    BTRY(b, cudaStreamSynchronize(st));
+    cudaFree(save);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    lbmgpu_batch_set_tiling(b, btx, bbps);
+    if (threads_per_row) *threads_per_row = btx;
+    if (ctas_per_sm) *ctas_per_sm = bbps;
+    if (best_ms) *best_ms = best;
+    return batch_status(b);
+}
+
+int lbmgpu_batch_time_bulk(lbmgpu_batch* b, int reps, double* ms_per_launch) {
+    if (!b || reps < 1 || !ms_per_launch) return LBMGPU_ERR_INVALID;
+    BTRY(b, cudaSetDevice(b->p0.device));
+    cudaStream_t st = b->sa;
+    BTRY(b, cudaStreamSynchronize(b->sb));
+    cudaEvent_t e0, e1;
+    BTRY(b, cudaEventCreate(&e0));
+    BTRY(b, cudaEventCreate(&e1));
+    const BatchStep bst{(int)((b->t + 1) % ZONE_SLOTS), 0, 0};
+    const int grid = b->sms * b->bps;
+    BTRY(b, cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) {
+        b->lz->batch_bulk((int)((b->t + 2 * r) & 1), false, false, b->tx, grid, b->ba, bst, st);
+        b->lz->batch_bulk((int)((b->t + 2 * r + 1) & 1), false, false, b->tx, grid, b->ba, bst, st);
+    }
+    BTRY(b, cudaEventRecord(e1, st));
+    BTRY(b, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    BTRY(b, cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->launches += 2 * reps;
+    *ms_per_launch = ms / (2.0 * reps);
+    return batch_status(b);
+}
+
+int lbmgpu_batch_set_stream(lbmgpu_batch* b, void* cuda_stream) {
+    if (!b) return LBMGPU_ERR_INVALID;
+    BTRY(b, cudaStreamSynchronize(b->sa));
+    b->sa = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : b->own;
+    for (lbmgpu_handle* h : b->m) h->stream = b->sa;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_batch_launch_count(const lbmgpu_batch* b, long long* n) {
+    if (!b || !n) return LBMGPU_ERR_INVALID;
+    *n = b->launches;
+    return LBMGPU_OK;
+}
+
+const char* lbmgpu_batch_last_error(const lbmgpu_batch* b) {
+    if (!b) return g_create_error.c_str();
+    return b->err.c_str();
 }
 
 }  // extern "C"

@@ -1,0 +1,104 @@
+"""Ensembles of independent lattices advanced together (lbmgpu_batch_* of
+include/lbmgpu.h).
+
+The reference runs one lattice per process (src/main.cpp); a parameter study
+there is one process per case (postprocessing/lbm_post.py:39-56). ``Ensemble``
+holds many cases on one GPU and advances all of them with one persistent bulk
+launch, one zone launch and one squirmer launch per time step, captured in
+CUDA graphs. Each member computes exactly what ``Solver(params).run(n)``
+computes for it alone; ``member(i)`` returns a read-only ``Solver`` view for
+its squirmer state, trajectory rows, fields and diagnostics.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+from ._lib import LbmgpuParams, check_batch
+from .params import Params
+from .solver import Solver
+
+
+class Ensemble:
+    def __init__(self, members: list[Params], autotune: bool = False, tune_reps: int = 5):
+        if not members:
+            raise ValueError("an ensemble needs at least one member")
+        for p in members:
+            p.validate()
+        self.params = list(members)
+        self.lib = _lib.load()
+        arr = (LbmgpuParams * len(members))(*[p.to_c() for p in members])
+        b = ctypes.c_void_p()
+        check_batch(self.lib.lbmgpu_batch_create(arr, len(members), ctypes.byref(b)), None)
+        self.b = b
+        self._views: dict[int, Solver] = {}
+        self.tiling = None
+        if autotune:
+            self.autotune(tune_reps)
+
+    def __len__(self) -> int:
+        return len(self.params)
+
+    @property
+    def cells(self) -> int:
+        n = ctypes.c_int()
+        c = ctypes.c_longlong()
+        check_batch(self.lib.lbmgpu_batch_size(self.b, ctypes.byref(n), ctypes.byref(c)), self.b)
+        return c.value
+
+    def run(self, nsteps: int) -> None:
+        check_batch(self.lib.lbmgpu_batch_run(self.b, int(nsteps)), self.b)
+
+    def member(self, i: int) -> Solver:
+        if i not in self._views:
+            h = ctypes.c_void_p()
+            check_batch(self.lib.lbmgpu_batch_member(self.b, int(i), ctypes.byref(h)), self.b)
+            self._views[i] = Solver._member(self.params[i], h, self)
+        return self._views[i]
+
+    def set_tiling(self, threads_per_row: int, ctas_per_sm: int) -> None:
+        check_batch(self.lib.lbmgpu_batch_set_tiling(self.b, int(threads_per_row), int(ctas_per_sm)), self.b)
+        self.tiling = (threads_per_row, ctas_per_sm)
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Chooses the bulk launch's tiling by timing every candidate; the
+        members' populations are restored afterwards."""
+        tx, bps = ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_double()
+        check_batch(self.lib.lbmgpu_batch_autotune(self.b, int(reps), ctypes.byref(tx), ctypes.byref(bps),
+                                                   ctypes.byref(ms)), self.b)
+        self.tiling = (tx.value, bps.value)
+        return dict(threads_per_row=tx.value, ctas_per_sm=bps.value, ms=ms.value)
+
+    def time_bulk(self, reps: int = 10) -> float:
+        ms = ctypes.c_double()
+        check_batch(self.lib.lbmgpu_batch_time_bulk(self.b, int(reps), ctypes.byref(ms)), self.b)
+        return ms.value
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        check_batch(self.lib.lbmgpu_batch_set_stream(self.b, ctypes.c_void_p(stream_handle or 0)), self.b)
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        check_batch(self.lib.lbmgpu_batch_launch_count(self.b, ctypes.byref(v)), self.b)
+        return v.value
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            for v in self._views.values():
+                v.h = None
+            self._views.clear()
+            self.lib.lbmgpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

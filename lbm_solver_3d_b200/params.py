@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import dataclasses
 from dataclasses import dataclass, field, fields
 from pathlib import Path
 
@@ -153,6 +154,9 @@ class Params:
                 raise ParamError(f"unknown parameter '{k}'")
         except ValueError:
             raise ParamError(f"invalid value '{v}' for parameter '{k}'") from None
+
+    def copy(self) -> "Params":
+        return dataclasses.replace(self)
 
     def update(self, **kv) -> "Params":
         for k, v in kv.items():

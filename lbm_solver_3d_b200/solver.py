@@ -31,6 +31,21 @@ class Solver:
         h = ctypes.c_void_p()
         check(self.lib.lbmgpu_create(ctypes.byref(c), ctypes.byref(h)), None)
         self.h = h
+        self._owned = True
+
+    @classmethod
+    def _member(cls, params: Params, handle: ctypes.c_void_p, owner) -> "Solver":
+        """View of a lattice owned by an ensemble (lbmgpu_batch_member): the
+        read-only calls work, the ensemble advances it and frees it."""
+        s = cls.__new__(cls)
+        s.params = params
+        s.lib = _lib.load()
+        s.N = params.ncells
+        s.shape = (params.NZ, params.NY, params.NX)
+        s.h = handle
+        s._owned = False
+        s._owner = owner
+        return s
 
     # ---- the reference's three per-step calls ----
     def step(self) -> None:
@@ -118,7 +133,8 @@ class Solver:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.lib.lbmgpu_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.lbmgpu_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -82,3 +82,23 @@ def test_null_handles_are_rejected():
     assert lib.lbmgpu_run(None, 1) == -1
     assert lib.lbmgpu_step(None) == -1
     assert lib.lbmgpu_destroy(None) == 0
+
+
+def test_ensemble_create_rejects_mixed_or_bad_members():
+    """lbmgpu_batch_create checks every member before touching the device."""
+    lib = _lib.load()
+    b = ctypes.c_void_p()
+    base = dict(nx=40, ny=26, nz=22, squirmer=1, radius=4.0)
+    cases = [
+        ([dict(base), dict(base, tau=0.9)], "members must share tau"),
+        ([dict(base), dict(base, nx=300)], "nx must be <= 256"),
+        ([dict(base), dict(base, tau=0.4)], "member 1: tau must be > 0.5"),
+    ]
+    for members, msg in cases:
+        arr = (_lib.LbmgpuParams * len(members))(*[Params().update(**m).to_c() for m in members])
+        assert lib.lbmgpu_batch_create(arr, len(members), ctypes.byref(b)) == -1
+        assert msg in lib.lbmgpu_batch_last_error(None).decode()
+        assert not b.value
+    assert lib.lbmgpu_batch_create(None, 0, ctypes.byref(b)) == -1
+    assert lib.lbmgpu_batch_run(None, 1) == -1
+    assert lib.lbmgpu_batch_destroy(None) == 0
