@@ -182,6 +182,39 @@ const char* lbmgpu_last_error(const lbmgpu_handle* h);
 int lbmgpu_abi_version(void);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free diagnostics (no counterpart in the reference: its
+ * diagnostics, lbm.cpp:342-364, read the solver's own host arrays).
+ *
+ * lbmgpu_field_stats_static computes what lbmgpu_diag reports (count of FLUID
+ * nodes, mean density, max |u| and sum of u_x over FLUID nodes) for fields
+ * that live in the CALLER's device memory: flag (N bytes, LBMGPU_FLUID = 0 in
+ * the low two bits), rho, ux, uy, uz (N doubles each), all on the current
+ * device. wall_force is not computed and is returned as 0.
+ *
+ * Who needs it: callers that keep their own lattice fields on the GPU and
+ * cannot allocate when they want the statistics. Creating a handle allocates
+ * about 100 bytes per node. cudaMalloc/cudaFree may synchronise the whole
+ * device and fail once HBM is committed to the populations. Code that must not
+ * stall other streams, or that runs with the memory already spoken for (a
+ * monitor polling a running time loop, a caller near the memory limit),
+ * therefore uses this entry point. It allocates no device memory: its reduction
+ * scratch is a static device array of the library (512 KB per device).
+ *
+ * Limit: 1 <= n_nodes <= LBMGPU_STATIC_STATS_MAX_NODES (2^25 nodes, e.g.
+ * 256^3 x 2); larger sizes return LBMGPU_ERR_INVALID with a message.
+ * Set-up: the first call on each device looks up the scratch's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Concurrency: the scratch is one per device and shared by all callers, so
+ * calls that overlap on a device (from several host threads, or on several
+ * streams) race and corrupt each other's results: serialise them.
+ * The call queues its work on cuda_stream (NULL: the legacy default stream)
+ * and returns after that stream has finished it. Errors are reported by
+ * lbmgpu_last_error(NULL) on the calling thread. */
+#define LBMGPU_STATIC_STATS_MAX_NODES 33554432LL
+int lbmgpu_field_stats_static(const uint8_t* flag, const double* rho, const double* ux, const double* uy,
+                              const double* uz, long long n_nodes, void* cuda_stream, lbmgpu_diagnostics* out);
+
+/* ---------------------------------------------------------------------------
  * Ensembles (no counterpart in the reference, whose executable runs one
  * lattice per process; parameter studies there launch the binary once per
  * case, e.g. postprocessing/lbm_post.py:39-56 driving src/main.cpp).

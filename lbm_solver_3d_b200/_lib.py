@@ -77,6 +77,8 @@ SIGNATURES = {
     "lbmgpu_time_kernels": (_I, [_P, _I, _DP]),
     "lbmgpu_last_error": (ctypes.c_char_p, [_P]),
     "lbmgpu_abi_version": (_I, []),
+    "lbmgpu_field_stats_static": (_I, [_P, _P, _P, _P, _P, ctypes.c_longlong, _P,
+                                       ctypes.POINTER(LbmgpuDiagnostics)]),
     "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
     "lbmgpu_batch_destroy": (_I, [_P]),
     "lbmgpu_batch_run": (_I, [_P, _I]),

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1535,3 +1536,137 @@ const char* lbmgpu_batch_last_error(const lbmgpu_batch* b) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+//  lbmgpu_field_stats_static: the diagnostics of lbmgpu_diag over fields in the
+//  caller's own device memory, with no allocation. Its reduction scratch is a
+//  file-scope device array (one per device, shared by every caller), not a
+//  handle buffer and not cudaMalloc.
+// ============================================================================
+namespace {
+
+constexpr int STATS_BLOCK = 256;
+constexpr int STATS_TILE = 2048;                                  // nodes per CTA (8 per thread)
+constexpr long long STATS_MAX_TILES = LBMGPU_STATIC_STATS_MAX_NODES / STATS_TILE;
+static_assert(LBMGPU_STATIC_STATS_MAX_NODES % STATS_TILE == 0, "tile count");
+
+// [0, 4*MAX_TILES)  per-tile partials (count, sum rho, max |u|, sum ux)
+// [4*MAX_TILES, +4) the result
+// then one unsigned completion counter (must be 0 at launch)
+struct StatsScratch {
+    double part[4 * STATS_MAX_TILES];
+    double result[4];
+    unsigned done;
+};
+static __device__ __align__(256) unsigned char g_stats_scratch[sizeof(StatsScratch)];   // 512 KB + 40 B per device
+
+// One CTA per tile of STATS_TILE nodes; the last CTA to finish sums the tile
+// partials in tile order, so the result does not depend on which CTAs ran first.
+__global__ void __launch_bounds__(STATS_BLOCK) k_field_stats_static(unsigned long long N, const uint8_t* flag,
+                                                                   const double* rho, const double* ux,
+                                                                   const double* uy, const double* uz,
+                                                                   StatsScratch* sc) {
+    __shared__ double red[STATS_BLOCK / 32][4];
+    __shared__ bool last;
+    double c = 0, m = 0, mx = 0, sx = 0;
+    const unsigned long long base = (unsigned long long)blockIdx.x * STATS_TILE;
+    for (int k = threadIdx.x; k < STATS_TILE; k += STATS_BLOCK) {
+        const unsigned long long n = base + k;
+        if (n >= N || (flag[n] & TYPE_MASK) != T_FLUID) continue;
+        c += 1.0; m += rho[n]; sx += ux[n];
+        mx = fmax(mx, sqrt(ux[n] * ux[n] + uy[n] * uy[n] + uz[n] * uz[n]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, o);
+        m += __shfl_down_sync(0xffffffffu, m, o);
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[w][0] = c; red[w][1] = m; red[w][2] = mx; red[w][3] = sx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, d = 0, e = 0;
+        for (int k = 0; k < STATS_BLOCK / 32; ++k) { a += red[k][0]; b += red[k][1]; d = fmax(d, red[k][2]); e += red[k][3]; }
+        double* p = sc->part + 4 * (size_t)blockIdx.x;
+        p[0] = a; p[1] = b; p[2] = d; p[3] = e;
+        __threadfence();
+        last = atomicAdd(&sc->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last CTA: strided sums over the tiles, then the same tree as above
+    c = m = mx = sx = 0;
+    for (unsigned t = threadIdx.x; t < gridDim.x; t += STATS_BLOCK) {
+        const volatile double* p = sc->part + 4 * (size_t)t;
+        c += p[0]; m += p[1]; mx = fmax(mx, p[2]); sx += p[3];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, o);
+        m += __shfl_down_sync(0xffffffffu, m, o);
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) { red[w][0] = c; red[w][1] = m; red[w][2] = mx; red[w][3] = sx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, d = 0, e = 0;
+        for (int k = 0; k < STATS_BLOCK / 32; ++k) { a += red[k][0]; b += red[k][1]; d = fmax(d, red[k][2]); e += red[k][3]; }
+        sc->result[0] = a; sc->result[1] = b; sc->result[2] = d; sc->result[3] = e;
+    }
+}
+
+// Device address of g_stats_scratch, looked up once per device.
+constexpr int STATS_MAX_DEVICES = 64;
+std::mutex g_stats_mu;
+StatsScratch* g_stats_addr[STATS_MAX_DEVICES] = {};
+
+cudaError_t stats_scratch(int dev, StatsScratch** out) {
+    std::lock_guard<std::mutex> lk(g_stats_mu);
+    if (!g_stats_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_stats_scratch);
+        if (e != cudaSuccess) return e;
+        g_stats_addr[dev] = static_cast<StatsScratch*>(p);
+    }
+    *out = g_stats_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int lbmgpu_field_stats_static(const uint8_t* flag, const double* rho, const double* ux, const double* uy,
+                                         const double* uz, long long n_nodes, void* cuda_stream,
+                                         lbmgpu_diagnostics* out) {
+    if (!out || !flag || !rho || !ux || !uy || !uz)
+        return fail(nullptr, LBMGPU_ERR_INVALID, "lbmgpu_field_stats_static: null pointer argument");
+    if (n_nodes < 1 || n_nodes > LBMGPU_STATIC_STATS_MAX_NODES)
+        return fail(nullptr, LBMGPU_ERR_INVALID,
+                    "lbmgpu_field_stats_static: n_nodes = " + std::to_string(n_nodes) + " is outside 1.." +
+                        std::to_string(LBMGPU_STATIC_STATS_MAX_NODES) + ", the capacity of its static scratch");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess && (dev < 0 || dev >= STATS_MAX_DEVICES)) e = cudaErrorInvalidDevice;
+    StatsScratch* sc = nullptr;
+    if (e == cudaSuccess) e = stats_scratch(dev, &sc);
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&sc->done, 0, sizeof(unsigned), st);
+    const unsigned tiles = (unsigned)((n_nodes + STATS_TILE - 1) / STATS_TILE);
+    if (e == cudaSuccess) {
+        k_field_stats_static<<<tiles, STATS_BLOCK, 0, st>>>((unsigned long long)n_nodes, flag, rho, ux, uy, uz, sc);
+        e = cudaGetLastError();
+    }
+    double r[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r, sc->result, sizeof(r), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(nullptr, LBMGPU_ERR_CUDA, std::string("lbmgpu_field_stats_static: ") + cudaGetErrorString(e));
+    out->n_fluid = (long long)r[0];
+    out->mean_density = r[0] > 0 ? r[1] / r[0] : 0.0;
+    out->max_speed = r[2];
+    out->sum_ux = r[3];
+    out->wall_force[0] = out->wall_force[1] = out->wall_force[2] = 0.0;
+    return LBMGPU_OK;
+}

@@ -102,3 +102,16 @@ def test_ensemble_create_rejects_mixed_or_bad_members():
     assert lib.lbmgpu_batch_create(None, 0, ctypes.byref(b)) == -1
     assert lib.lbmgpu_batch_run(None, 1) == -1
     assert lib.lbmgpu_batch_destroy(None) == 0
+
+
+def test_static_stats_checks_arguments_before_touching_the_device():
+    """lbmgpu_field_stats_static rejects null pointers and sizes beyond its
+    static scratch (2^25 nodes) with a message, before any CUDA call."""
+    lib = _lib.load()
+    d = _lib.LbmgpuDiagnostics()
+    fake = ctypes.c_void_p(256)   # never dereferenced
+    assert lib.lbmgpu_field_stats_static(None, fake, fake, fake, fake, 10, None, ctypes.byref(d)) == -1
+    assert b"null pointer" in lib.lbmgpu_last_error(None)
+    for n in (0, -5, (1 << 25) + 1):
+        assert lib.lbmgpu_field_stats_static(fake, fake, fake, fake, fake, n, None, ctypes.byref(d)) == -1
+        assert b"33554432, the capacity of its static scratch" in lib.lbmgpu_last_error(None)
