@@ -67,6 +67,7 @@ class ClockSampler:
 
     def __init__(self, gpu: int):
         self.gpu, self.rows, self.proc = gpu, [], None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -75,13 +76,22 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            deadline = time.time() + 5.0      # the timed region starts once sampling runs
+            while not self.rows and time.time() < deadline:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            self.rows.append((time.time(), [c.strip() for c in line.split(",")]))
+
+    def start(self):
+        self.t0 = time.time()
+
+    def stop(self):
+        self.t1 = time.time()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -92,14 +102,19 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        rows = self.rows
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for t, r in rows if self.t0 <= t <= self.t1 + 0.2]
+        else:
+            inside = [r for _, r in rows]
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        reasons = sorted({names[k] for r in inside for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(inside)}
 
 
 def cpu_baseline(p, seconds_target=15.0):
@@ -138,23 +153,27 @@ def run_reference_arm(args, p):
     oracle.set_threads(threads)
     kind = "reference" if oracle.ref_available() else "port"
     s = oracle.RefSolver(p) if kind == "reference" else oracle.PortSolver(p)
-    for _ in range(args.warmup):
+    # a bounded sample of the workload: at most K steps and about 90 s of CPU time
+    warm = min(args.warmup, 3)
+    for _ in range(warm):
         s.run(1)
     times = []
-    for _ in range(args.steps):
+    budget = 90.0
+    while len(times) < args.steps and sum(times) < budget:
         t0 = time.perf_counter()
         s.run(1)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
-    mlups = p.ncells * args.steps / tot / 1e6
+    n = len(times)
+    mlups = p.ncells * n / tot / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / n,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(args, p, reference=True),
         "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
-                         "sample": f"{args.steps} time steps of the workload after {args.warmup} warm-up steps, "
-                                   f"{threads} OpenMP threads"},
+                         "sample": f"{n} of the workload's time steps (bounded to ~{budget:.0f} s) after {warm} "
+                                   f"warm-up steps, {threads} OpenMP threads"},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -199,11 +218,13 @@ def bench_ensemble(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = ens.launch_count()
     with ClockSampler(local) as clk:
+        clk.start()
         with torch.cuda.stream(stream):
             ev0.record(stream)
             ens.run(args.steps)
             ev1.record(stream)
         torch.cuda.synchronize()
+        clk.stop()
     ms_step = ev0.elapsed_time(ev1) / args.steps
     launches = ens.launch_count() - l0
     bulk_ms = ens.time_bulk(reps=5)
@@ -259,8 +280,8 @@ def bench_ensemble(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--precision", default="fp32", choices=list(BYTES))
     ap.add_argument("--workload", default="bulk_0")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -304,11 +325,13 @@ def main():
         pg.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        clk.start()
         with torch.cuda.stream(stream):
             ev0.record(stream)
             sol.run(args.steps)
             ev1.record(stream)
         torch.cuda.synchronize()
+        clk.stop()
     if pg:
         pg.barrier()
     ms = ev0.elapsed_time(ev1)
