@@ -182,6 +182,45 @@ const char* lbmgpu_last_error(const lbmgpu_handle* h);
 int lbmgpu_abi_version(void);
 
 /* ---------------------------------------------------------------------------
+ * Swimmer surrogate network (no counterpart in the reference).
+ *
+ * A multilayer perceptron 4 -> 64 -> 64 -> 64 -> 3 with SiLU after each
+ * hidden layer, trained and evaluated by the library's own kernels: one CTA
+ * runs the whole network forward and backward on a tile of 32 samples, and a
+ * second kernel sums the tiles' gradients in a fixed order and takes one
+ * Adam step on the FP32 master parameters. With bf16 = 1 every matrix product
+ * uses BF16 operands on the tensor cores with FP32 accumulation; with bf16 = 0
+ * it is computed in FP32.
+ * Parameters (LBMGPU_MLP_NPARAMS floats): W1[64][4] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] W4[3][64] b4[3], each W[out][in]. Loss: mean over samples
+ * and outputs of the squared error. Inputs x[n][4], targets/outputs y[n][3],
+ * FP32, row-major. Errors: lbmgpu_mlp_last_error.
+ * ------------------------------------------------------------------------- */
+#define LBMGPU_MLP_IN 4
+#define LBMGPU_MLP_HIDDEN 64
+#define LBMGPU_MLP_OUT 3
+#define LBMGPU_MLP_NPARAMS (64 * 4 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 3 * 64 + 3)
+typedef struct lbmgpu_mlp lbmgpu_mlp;
+int lbmgpu_mlp_create(int device, int bf16, lbmgpu_mlp** out);   /* parameters 0 */
+int lbmgpu_mlp_destroy(lbmgpu_mlp* m);
+int lbmgpu_mlp_set_params(lbmgpu_mlp* m, const float* params, int reset_optimizer);
+int lbmgpu_mlp_get_params(lbmgpu_mlp* m, float* params);
+/* Adam hyper-parameters (defaults 0.9, 0.999, 1e-8). */
+int lbmgpu_mlp_set_adam(lbmgpu_mlp* m, float beta1, float beta2, float eps);
+/* Training set, copied to the device. */
+int lbmgpu_mlp_set_data(lbmgpu_mlp* m, const float* x, const float* y, int n);
+/* Adam steps over consecutive minibatches of `batch` samples taken from the
+ * training set in the given order (indices into the training set); returns
+ * the mean of the minibatch losses in *mean_loss (may be NULL). */
+int lbmgpu_mlp_train_epoch(lbmgpu_mlp* m, const int* order, int n_order, int batch, float lr, float* mean_loss);
+/* Loss and gradient (LBMGPU_MLP_NPARAMS floats, may be NULL) over the whole
+ * training set at the current parameters; no update. */
+int lbmgpu_mlp_loss_grad(lbmgpu_mlp* m, float* loss, float* grad);
+/* Inference: y[n][3] = net(x[n][4]). */
+int lbmgpu_mlp_forward(lbmgpu_mlp* m, const float* x, int n, float* y);
+const char* lbmgpu_mlp_last_error(const lbmgpu_mlp* m);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free diagnostics (no counterpart in the reference: its
  * diagnostics, lbm.cpp:342-364, read the solver's own host arrays).
  *

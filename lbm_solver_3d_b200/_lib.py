@@ -79,6 +79,17 @@ SIGNATURES = {
     "lbmgpu_abi_version": (_I, []),
     "lbmgpu_field_stats_static": (_I, [_P, _P, _P, _P, _P, ctypes.c_longlong, _P,
                                        ctypes.POINTER(LbmgpuDiagnostics)]),
+    "lbmgpu_mlp_create": (_I, [_I, _I, ctypes.POINTER(_P)]),
+    "lbmgpu_mlp_destroy": (_I, [_P]),
+    "lbmgpu_mlp_set_params": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I]),
+    "lbmgpu_mlp_get_params": (_I, [_P, ctypes.POINTER(ctypes.c_float)]),
+    "lbmgpu_mlp_set_adam": (_I, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
+    "lbmgpu_mlp_set_data": (_I, [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _I]),
+    "lbmgpu_mlp_train_epoch": (_I, [_P, ctypes.POINTER(ctypes.c_int), _I, _I, ctypes.c_float,
+                                    ctypes.POINTER(ctypes.c_float)]),
+    "lbmgpu_mlp_loss_grad": (_I, [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "lbmgpu_mlp_forward": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float)]),
+    "lbmgpu_mlp_last_error": (ctypes.c_char_p, [_P]),
     "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
     "lbmgpu_batch_destroy": (_I, [_P]),
     "lbmgpu_batch_run": (_I, [_P, _I]),
