@@ -90,6 +90,12 @@ def main():
     e_s = np.array([m["err_surrogate"] for m in per_member])
     e_b = np.array([m["err_bulk_speed"] for m in per_member])
     trusted = np.array([m["trusted"] for m in per_member])
+    by_tol = {}
+    for tol in (0.02, 0.03, 0.05, 0.1):
+        pm, _ = evaluate(s, htable, hrows, args.transient, tol=tol)
+        tr = np.array([m["trusted"] for m in pm])
+        by_tol[str(tol)] = {"trusted_members": int(tr.sum()),
+                            "max_err_trusted": float(e_s[tr].max()) if tr.any() else None}
     dgen = np.load(d / "surrogate_heldout.npz")
     report = {
         "samples_train": int((~vmask).sum()) * 2, "samples_val": int(vmask.sum()),
@@ -105,6 +111,7 @@ def main():
                                                   "max": float(e_b.max()),
                                                   "within_5pct": int((e_b <= 0.05).sum())},
         "trusted_members": int(trusted.sum()),
+        "trust_tolerance_sweep": by_tol,
         "drift_rel_err_trusted_only": {"max": float(e_s[trusted].max()) if trusted.any() else None,
                                        "median": float(np.median(e_s[trusted])) if trusted.any() else None},
         "time_surrogate_s": t_sur,

@@ -98,6 +98,7 @@ def run_duct_to_convergence(solver, p):
     return t, False
 
 
+@pytest.mark.slow
 def test_port_reproduces_shipped_duct_summary(port):
     p = deck(DUCT)
     s = port(p)
@@ -118,6 +119,7 @@ def test_port_reproduces_shipped_duct_summary(port):
     assert np.allclose(exact, prof[:, 2], rtol=1e-9)
 
 
+@pytest.mark.slow
 def test_port_matches_full_duct_fixture(port):
     """The duct workload (16x32x32, 20000 steps) against the reference's own run."""
     g = np.load(GOLDEN / "ref_duct.npz")
