@@ -289,15 +289,22 @@ int lbmgpu_batch_member(lbmgpu_batch* b, int i, lbmgpu_handle** h);
 /* Number of members and total lattice nodes (either pointer may be NULL). */
 int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
 
-/* Tiling of the bulk launch: threads_per_row (32, 64 or 128 threads cover
- * one x-row) and ctas_per_sm (1..16; the grid is that many CTAs per SM). */
-int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int threads_per_row, int ctas_per_sm);
+/* Tiling of the bulk launch. tile = 32, 64 or 128: every CTA walks rows with
+ * that many threads per x-row, loading populations straight from global
+ * memory. tile = LBMGPU_TILE_ROWCTA: one CTA of 128 threads per row. tile = LBMGPU_TILE_STAGED2 / _STAGED3: each CTA owns a contiguous
+ * range of rows (equal node counts) and stages every row's populations in
+ * shared memory with bulk asynchronous copies, 2 or 3 rows deep.
+ * ctas_per_sm (1..16): the grid is that many CTAs per SM. */
+#define LBMGPU_TILE_ROWCTA 1     /* one CTA per row, grid = rows (ctas_per_sm unused) */
+#define LBMGPU_TILE_STAGED2 (-2)
+#define LBMGPU_TILE_STAGED3 (-3)
+int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm);
 
 /* Times the bulk launch for every tiling candidate, `reps` pairs of launches
  * each, and keeps the fastest. The populations are saved to a temporary
  * device buffer before and restored after, so the ensemble's state is
  * unchanged. Outputs (may be NULL): the chosen tiling and its time per launch. */
-int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* ctas_per_sm, double* best_ms);
+int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* tile, int* ctas_per_sm, double* best_ms);
 
 /* Measurement aid: average device time of one bulk launch over all members
  * with the current tiling (2*reps launches; the populations advance without

@@ -168,9 +168,21 @@ __device__ __forceinline__ bool wall_dir(int i, uint8_t wr) {
     return (CY(i) < 0 && (wr & 1)) || (CY(i) > 0 && (wr & 2)) || (CZ(i) < 0 && (wr & 4)) || (CZ(i) > 0 && (wr & 8));
 }
 
-template <class S, int PAR, bool GENERAL, bool MACRO>
+// Where update_node reads the 19 logical populations from: the population
+// array itself (GlobalSrc), or a copy staged in shared memory (StagedSrc in
+// k_batch.cuh). Either returns the stored values converted by S::ld.
+struct GlobalSrc {
+    template <class S, int PAR, class V>
+    __device__ __forceinline__ void load(const typename S::T* __restrict__ f, unsigned N, unsigned n, const Nbr& nb,
+                                         V* v) const {
+        load_node<S, PAR>(f, N, n, nb, v);
+    }
+};
+
+template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
-                                            uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out) {
+                                            uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
+                                            const Src& src = Src()) {
     using T = typename S::T;
     T* __restrict__ f = static_cast<T*>(a.f);
     const unsigned N = L.N;
@@ -184,7 +196,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
     if constexpr (!S::shifted) {
         // ---------------- FP64: the reference's arithmetic ----------------
         double fv[Q];
-        load_node<S, PAR>(f, N, n, nb, fv);
+        src.template load<S, PAR>(f, N, n, nb, fv);
         if (a.apply_corr) {
             const double corr = sq->corr_d;
 #pragma unroll
@@ -251,7 +263,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
     } else {
         // ------------- FP32 arithmetic on stored deviations ---------------
         float d[Q];
-        load_node<S, PAR>(f, N, n, nb, d);
+        src.template load<S, PAR>(f, N, n, nb, d);
         if (a.apply_corr) {
             const double corr = sq->corr_d;
 #pragma unroll

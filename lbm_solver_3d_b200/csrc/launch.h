@@ -34,6 +34,8 @@ struct BatchArgs {
     int gzmax;                         // zone blocks per member (grid x of the zone launch)
     int nmembers;
     const MemberParts* parts;
+    const int* bounds;                 // staged kernel: row range of each CTA (grid + 1 entries)
+    int cap;                           // staged kernel: elements per staged direction-row
 };
 
 struct Launchers {
@@ -59,6 +61,11 @@ struct Launchers {
     void (*batch_bulk)(int par, bool macro, bool wallrows, int tx, int grid, const BatchArgs& b, BatchStep st,
                        cudaStream_t s);
     void (*batch_zone)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    // the rows away from walls through shared-memory stages (k_bulk_staged)
+    void (*batch_staged)(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    // the rows away from walls, one CTA per row (k_bulk_rowcta)
+    void (*batch_rowcta)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    size_t esize;
     void (*batch_squirmer)(const BatchArgs& b, SqStep st, cudaStream_t s);
 };
 

@@ -46,6 +46,7 @@ constexpr int ST_NAN = 1;            // non-finite force/torque/state
 constexpr int ST_REMAP_RANGE = 2;    // squirmer moved >= 1 cell in one step
 constexpr int ST_LINK_OVERFLOW = 4;  // boundary-link list exceeded its capacity
 constexpr int ST_REMAP_OVERFLOW = 8; // more changed nodes than the remap can order
+constexpr int ST_WATCHDOG = 16;      // a bounded wait for staged data gave up
 
 // ---- storage forms ----------------------------------------------------------
 // FP64: f_i itself. FP32 / FP16: the deviation f_i - w_i rho0 (rho0 = 1), FP16

@@ -104,6 +104,47 @@ static void batch_bulk_launch(int par, bool macro, bool wr, int tx, int grid, co
 }
 
 template <class S>
+static void batch_rowcta_launch(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    if (b.nrows == 0) return;
+    switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
+        case 0: k_bulk_rowcta<S, 0, false><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
+        case 1: k_bulk_rowcta<S, 0, true><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
+        case 2: k_bulk_rowcta<S, 1, false><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
+        default: k_bulk_rowcta<S, 1, true><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
+    }
+}
+
+template <class S, int PAR, bool MACRO, int NST>
+static void staged_one(int grid, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    const size_t smem = (size_t)NST * Q * b.cap * sizeof(typename S::T);
+    k_bulk_staged<S, PAR, MACRO, NST><<<grid, STAGED_THREADS, smem, s>>>(b.lat, b.args, b.rows, b.bounds, b.row_part,
+                                                                        st, b.cap);
+}
+
+template <class S>
+static void batch_staged_launch(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st,
+                                cudaStream_t s) {
+    if (b.nrows == 0) return;
+    const int sel = (par ? 4 : 0) | (macro ? 2 : 0) | (nst == 3 ? 1 : 0);
+    switch (sel) {
+        case 0: staged_one<S, 0, false, 2>(grid, b, st, s); break;
+        case 1: staged_one<S, 0, false, 3>(grid, b, st, s); break;
+        case 2: staged_one<S, 0, true, 2>(grid, b, st, s); break;
+        case 3: staged_one<S, 0, true, 3>(grid, b, st, s); break;
+        case 4: staged_one<S, 1, false, 2>(grid, b, st, s); break;
+        case 5: staged_one<S, 1, false, 3>(grid, b, st, s); break;
+        case 6: staged_one<S, 1, true, 2>(grid, b, st, s); break;
+        default: staged_one<S, 1, true, 3>(grid, b, st, s); break;
+    }
+}
+
+template <class S, int PAR, bool MACRO, int NST>
+static cudaError_t staged_attr() {
+    return cudaFuncSetAttribute(k_bulk_staged<S, PAR, MACRO, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                200 * 1024);
+}
+
+template <class S>
 static void batch_zone_launch(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s) {
     const dim3 grid(b.gzmax, b.nmembers);
     switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
@@ -123,7 +164,14 @@ template <class S>
 static cudaError_t prepare_launch() {
     cudaError_t e = cudaFuncSetAttribute(k_squirmer<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+    e = cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+    if (e != cudaSuccess) return e;
+    cudaError_t es[8] = {staged_attr<S, 0, false, 2>(), staged_attr<S, 0, false, 3>(), staged_attr<S, 0, true, 2>(),
+                         staged_attr<S, 0, true, 3>(),  staged_attr<S, 1, false, 2>(), staged_attr<S, 1, false, 3>(),
+                         staged_attr<S, 1, true, 2>(),  staged_attr<S, 1, true, 3>()};
+    for (cudaError_t x : es)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
 }
 
 template <class S>
@@ -141,6 +189,9 @@ static Launchers make_launchers() {
     l.batch_bulk = &batch_bulk_launch<S>;
     l.batch_zone = &batch_zone_launch<S>;
     l.batch_squirmer = &batch_squirmer_launch<S>;
+    l.batch_staged = &batch_staged_launch<S>;
+    l.batch_rowcta = &batch_rowcta_launch<S>;
+    l.esize = sizeof(typename S::T);
     return l;
 }
 

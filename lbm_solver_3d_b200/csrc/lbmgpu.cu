@@ -1096,7 +1096,13 @@ struct lbmgpu_batch {
     double *row_part = nullptr, *zone_part = nullptr;
     int* d_status = nullptr;
     BatchArgs ba{};
-    int tx = 32, bps = 4;          // tiling of the bulk launch (autotuned)
+    // tiling of the bulk launch (autotuned): tile > 0 is k_bulk_batch with that
+    // many threads per row, tile < 0 is k_bulk_staged with -tile stages;
+    // the grid is bps CTAs per SM
+    int tile = 32, bps = 4;
+    int* d_bounds = nullptr;       // staged kernel: row range of each CTA
+    int bounds_cap = 0, bounds_grid = 0;
+    std::vector<long long> row_prefix;   // nodes in the rows before row r (rows away from walls)
     long long cells = 0, t = 0, launches = 0;
     bool pending_corr = false;
     Graph g;
@@ -1128,7 +1134,7 @@ void batch_free(lbmgpu_batch* b) {
     }
     b->m.clear();
     void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts,
-                    b->row_part, b->zone_part, b->d_status};
+                    b->row_part, b->zone_part, b->d_status, b->d_bounds};
     for (void* q : ptrs) if (q) cudaFree(q);
     for (cudaEvent_t e : {b->ev_b[0], b->ev_b[1], b->ev_z, b->ev_s, b->ev_fork, b->ev_join})
         if (e) cudaEventDestroy(e);
@@ -1141,6 +1147,40 @@ bool is_corr_batch(const lbmgpu_batch* b, long long s) {
     return b->has_sq && k > 0 && s % k == 0;
 }
 
+// Row ranges of the staged kernel's CTAs: contiguous, with equal node counts.
+int set_bounds(lbmgpu_batch* b, int grid) {
+    if (b->bounds_grid == grid && b->d_bounds) return LBMGPU_OK;
+    if (grid + 1 > b->bounds_cap) {
+        if (b->d_bounds) cudaFree(b->d_bounds);
+        b->d_bounds = nullptr;
+        b->bounds_cap = 0;
+        BTRY(b, cudaMalloc(&b->d_bounds, (size_t)(grid + 1) * sizeof(int)));
+        b->bounds_cap = grid + 1;
+        b->ba.bounds = b->d_bounds;
+    }
+    const std::vector<long long>& pre = b->row_prefix;   // size nrows + 1
+    const int nrows = (int)pre.size() - 1;
+    std::vector<int> bd(grid + 1);
+    bd[0] = 0;
+    int r = 0;
+    for (int c = 1; c < grid; ++c) {
+        const long long target = pre[nrows] * c / grid;
+        while (r < nrows && pre[r] < target) ++r;
+        bd[c] = r;
+    }
+    bd[grid] = nrows;
+    BTRY(b, cudaMemcpy(b->d_bounds, bd.data(), (size_t)(grid + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    b->bounds_grid = grid;
+    return LBMGPU_OK;
+}
+
+// the bulk launch (rows away from walls) with a given tiling
+void launch_bulk(lbmgpu_batch* b, int tile, int grid, int par, bool macro, BatchStep bst, cudaStream_t s) {
+    if (tile < 0) b->lz->batch_staged(par, macro, -tile, grid, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, b->ba, bst, s);
+    else b->lz->batch_bulk(par, macro, false, tile, grid, b->ba, bst, s);
+}
+
 void issue_batch(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb, long long s, bool macro, bool apply,
                  bool capture = false) {
     const int par = (int)((s - 1) & 1);
@@ -1149,7 +1189,7 @@ void issue_batch(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb, long long s,
     const int grid = b->sms * b->bps;
     cudaStreamWaitEvent(sa, b->ev_z, 0);
     if (apply) cudaStreamWaitEvent(sa, b->ev_s, 0);
-    b->lz->batch_bulk(par, macro, false, b->tx, grid, b->ba, bst, sa);
+    launch_bulk(b, b->tile, grid, par, macro, bst, sa);
     cudaEventRecord(b->ev_b[s & 1], sa);
     cudaStreamWaitEvent(sb, b->ev_b[(s - 1) & 1], 0);
     int k = 1;
@@ -1214,6 +1254,7 @@ int batch_status(lbmgpu_batch* b) {
     BTRY(b, cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->sa));
     BTRY(b, cudaStreamSynchronize(b->sa));
     if (st & ST_NAN) return bfail(b, LBMGPU_ERR_NAN, "non-finite squirmer force, torque or state in a member");
+    if (st & ST_WATCHDOG) return bfail(b, LBMGPU_ERR_WATCHDOG, "a staged row did not arrive in shared memory in time");
     if (st & (ST_REMAP_RANGE | ST_LINK_OVERFLOW | ST_REMAP_OVERFLOW))
         return bfail(b, LBMGPU_ERR_DEVICE, "a member's squirmer update failed a consistency check");
     return LBMGPU_OK;
@@ -1356,10 +1397,19 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
     b->ba.wrows = b->d_wrows; b->ba.nwrows = (int)wrows.size();
     b->ba.row_part = b->row_part; b->ba.zone_part = b->zone_part;
     b->ba.gzmax = gzmax; b->ba.nmembers = n; b->ba.parts = b->d_parts;
+    {
+        int nxmax = 1;
+        for (int i = 0; i < n; ++i) nxmax = std::max(nxmax, ps[i].nx);
+        const size_t es = b->lz->esize;
+        b->ba.cap = (int)(((size_t)nxmax * es + 32 + 15) / 16 * 16 / es);
+        b->row_prefix.assign(rows.size() + 1, 0);
+        for (size_t r = 0; r < rows.size(); ++r) b->row_prefix[r + 1] = b->row_prefix[r] + ps[rows[r].m].nx;
+    }
     const int k = p0.mass_correction_every;
     const int base = std::lcm(2, ZONE_SLOTS);
     b->corr_in_graph = b->has_sq && k > 0 && std::lcm(base, k) <= MAX_PERIOD;
     b->period = b->corr_in_graph ? std::lcm(base, k) : base;
+    if (set_bounds(b, b->sms * b->bps) != LBMGPU_OK) return bail(LBMGPU_ERR_CUDA);
 #undef CB
     *out = b;
     return LBMGPU_OK;
@@ -1428,11 +1478,19 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
     return batch_status(b);
 }
 
-int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int threads_per_row, int ctas_per_sm) {
+int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (!b) return LBMGPU_ERR_INVALID;
-    if ((threads_per_row != 32 && threads_per_row != 64 && threads_per_row != 128) || ctas_per_sm < 1 || ctas_per_sm > 16)
-        return bfail(b, LBMGPU_ERR_INVALID, "threads_per_row must be 32, 64 or 128 and ctas_per_sm 1..16");
-    b->tx = threads_per_row;
+    if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED2 && tile != LBMGPU_TILE_STAGED3 &&
+         tile != LBMGPU_TILE_ROWCTA) ||
+        ctas_per_sm < 1 || ctas_per_sm > 16)
+        return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA or "
+                                            "LBMGPU_TILE_STAGED2/3, and ctas_per_sm 1..16");
+    BTRY(b, cudaSetDevice(b->p0.device));
+    BTRY(b, cudaStreamSynchronize(b->sa));
+    BTRY(b, cudaStreamSynchronize(b->sb));
+    const int rc = set_bounds(b, b->sms * ctas_per_sm);
+    if (rc) return rc;
+    b->tile = tile;
     b->bps = ctas_per_sm;
     if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
     if (b->g.graph) cudaGraphDestroy(b->g.graph);
@@ -1455,20 +1513,25 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaEvent_t e0, e1;
     BTRY(b, cudaEventCreate(&e0));
     BTRY(b, cudaEventCreate(&e1));
-    const int txs[3] = {32, 64, 128};
-    const int bpss[6] = {1, 2, 3, 4, 6, 8};
+    const int tiles[6] = {LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED2, LBMGPU_TILE_STAGED3};
+    const int bpss[7] = {1, 2, 3, 4, 5, 6, 8};
     double best = 1e30;
-    int btx = b->tx, bbps = b->bps;
+    int btx = b->tile, bbps = b->bps;
     const BatchStep bst{(int)((b->t + 1) % ZONE_SLOTS), 0, 0};
-    for (int tx : txs)
+    for (int tx : tiles)
         for (int bps : bpss) {
+            if (tx == LBMGPU_TILE_ROWCTA && bps != 1) continue;   // its grid is the row count
             const int grid = b->sms * bps;
-            b->lz->batch_bulk(0, false, false, tx, grid, b->ba, bst, st);  // warm-up
-            b->lz->batch_bulk(1, false, false, tx, grid, b->ba, bst, st);
+            if (tx < 0) {
+                const int rc = set_bounds(b, grid);
+                if (rc) return rc;
+            }
+            launch_bulk(b, tx, grid, 0, false, bst, st);  // warm-up
+            launch_bulk(b, tx, grid, 1, false, bst, st);
             BTRY(b, cudaEventRecord(e0, st));
             for (int r = 0; r < reps; ++r) {
-                b->lz->batch_bulk(0, false, false, tx, grid, b->ba, bst, st);
-                b->lz->batch_bulk(1, false, false, tx, grid, b->ba, bst, st);
+                launch_bulk(b, tx, grid, 0, false, bst, st);
+                launch_bulk(b, tx, grid, 1, false, bst, st);
             }
             BTRY(b, cudaEventRecord(e1, st));
             BTRY(b, cudaEventSynchronize(e1));
@@ -1483,7 +1546,8 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaFree(save);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    lbmgpu_batch_set_tiling(b, btx, bbps);
+    const int rc = lbmgpu_batch_set_tiling(b, btx, bbps);
+    if (rc) return rc;
     if (threads_per_row) *threads_per_row = btx;
     if (ctas_per_sm) *ctas_per_sm = bbps;
     if (best_ms) *best_ms = best;
@@ -1502,8 +1566,8 @@ int lbmgpu_batch_time_bulk(lbmgpu_batch* b, int reps, double* ms_per_launch) {
     const int grid = b->sms * b->bps;
     BTRY(b, cudaEventRecord(e0, st));
     for (int r = 0; r < reps; ++r) {
-        b->lz->batch_bulk((int)((b->t + 2 * r) & 1), false, false, b->tx, grid, b->ba, bst, st);
-        b->lz->batch_bulk((int)((b->t + 2 * r + 1) & 1), false, false, b->tx, grid, b->ba, bst, st);
+        launch_bulk(b, b->tile, grid, (int)((b->t + 2 * r) & 1), false, bst, st);
+        launch_bulk(b, b->tile, grid, (int)((b->t + 2 * r + 1) & 1), false, bst, st);
     }
     BTRY(b, cudaEventRecord(e1, st));
     BTRY(b, cudaEventSynchronize(e1));

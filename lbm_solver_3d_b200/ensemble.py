@@ -56,9 +56,13 @@ class Ensemble:
             self._views[i] = Solver._member(self.params[i], h, self)
         return self._views[i]
 
-    def set_tiling(self, threads_per_row: int, ctas_per_sm: int) -> None:
-        check_batch(self.lib.lbmgpu_batch_set_tiling(self.b, int(threads_per_row), int(ctas_per_sm)), self.b)
-        self.tiling = (threads_per_row, ctas_per_sm)
+    STAGED2, STAGED3 = -2, -3
+
+    def set_tiling(self, tile: int, ctas_per_sm: int) -> None:
+        """tile 32/64/128: threads per row of the row kernel; -2/-3: the staged
+        kernel with 2/3 shared-memory stages."""
+        check_batch(self.lib.lbmgpu_batch_set_tiling(self.b, int(tile), int(ctas_per_sm)), self.b)
+        self.tiling = (tile, ctas_per_sm)
 
     def autotune(self, reps: int = 5) -> dict:
         """Chooses the bulk launch's tiling by timing every candidate; the
@@ -68,7 +72,7 @@ class Ensemble:
         check_batch(self.lib.lbmgpu_batch_autotune(self.b, int(reps), ctypes.byref(tx), ctypes.byref(bps),
                                                    ctypes.byref(ms)), self.b)
         self.tiling = (tx.value, bps.value)
-        return dict(threads_per_row=tx.value, ctas_per_sm=bps.value, ms=ms.value)
+        return dict(tile=tx.value, ctas_per_sm=bps.value, ms=ms.value)
 
     def time_bulk(self, reps: int = 10) -> float:
         ms = ctypes.c_double()

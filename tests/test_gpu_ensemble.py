@@ -83,15 +83,19 @@ def test_ensemble_equals_members_alone(api, precision):
             assert_member_equals_alone(ens, i, p, Solver, [101, 129])
 
 
-@pytest.mark.parametrize("tiling", [(32, 1), (64, 3), (128, 8)])
+@pytest.mark.parametrize("tiling", [(32, 1), (64, 3), (128, 8), (1, 1), (-2, 4), (-3, 2), (-2, 16)])
 def test_ensemble_tiling_does_not_change_results(api, tiling):
+    """Row kernel (tile > 0 threads per row) and staged kernel (tile = -2, -3
+    stages), with few or many CTAs per SM: bit-identical to the lattices run
+    alone, in FP32 and FP64."""
     Ensemble, Solver = api
-    ps = members("fp32")
-    with Ensemble(ps) as ens:
-        ens.set_tiling(*tiling)
-        ens.run(60)
-        for i in (0, 4):
-            assert_member_equals_alone(ens, i, ps[i], Solver, [60])
+    for prec in ("fp32", "fp64"):
+        ps = members(prec)
+        with Ensemble(ps) as ens:
+            ens.set_tiling(*tiling)
+            ens.run(60)
+            for i in (0, 2, 4):
+                assert_member_equals_alone(ens, i, ps[i], Solver, [60])
 
 
 def test_ensemble_autotune_restores_state(api):
@@ -100,7 +104,7 @@ def test_ensemble_autotune_restores_state(api):
     with Ensemble(ps) as ens:
         ens.run(30)
         tuned = ens.autotune(reps=2)
-        assert tuned["threads_per_row"] in (32, 64, 128) and 1 <= tuned["ctas_per_sm"] <= 16
+        assert tuned["tile"] in (1, 32, 64, 128, -2, -3) and 1 <= tuned["ctas_per_sm"] <= 16
         assert tuned["ms"] > 0
         ens.run(40)
         for i in range(len(ps)):
