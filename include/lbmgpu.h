@@ -289,15 +289,19 @@ int lbmgpu_batch_member(lbmgpu_batch* b, int i, lbmgpu_handle** h);
 /* Number of members and total lattice nodes (either pointer may be NULL). */
 int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
 
-/* Tiling of the bulk launch. tile = 32, 64 or 128: every CTA walks rows with
- * that many threads per x-row, loading populations straight from global
- * memory. tile = LBMGPU_TILE_ROWCTA: one CTA of 128 threads per row. tile = LBMGPU_TILE_STAGED2 / _STAGED3: each CTA owns a contiguous
- * range of rows (equal node counts) and stages every row's populations in
- * shared memory with bulk asynchronous copies, 2 or 3 rows deep.
+/* Tiling of the bulk launch.
+ *   tile = 32, 64 or 128: every CTA walks rows with that many threads per
+ *     x-row, loading populations straight from global memory;
+ *   tile = LBMGPU_TILE_ROWCTA: one CTA of 128 threads per row (grid = rows,
+ *     ctas_per_sm unused);
+ *   tile = LBMGPU_TILE_STAGED3 / _STAGED4: each CTA owns a contiguous range
+ *     of rows (equal node counts); a producer warp stages every row's
+ *     populations and flags in shared memory with bulk asynchronous copies,
+ *     3 or 4 rows deep, while four warps update the rows already staged.
  * ctas_per_sm (1..16): the grid is that many CTAs per SM. */
-#define LBMGPU_TILE_ROWCTA 1     /* one CTA per row, grid = rows (ctas_per_sm unused) */
-#define LBMGPU_TILE_STAGED2 (-2)
+#define LBMGPU_TILE_ROWCTA 1
 #define LBMGPU_TILE_STAGED3 (-3)
+#define LBMGPU_TILE_STAGED4 (-4)
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm);
 
 /* Times the bulk launch for every tiling candidate, `reps` pairs of launches

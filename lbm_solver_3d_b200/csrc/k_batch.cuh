@@ -168,26 +168,35 @@ __global__ void __launch_bounds__(ROWCTA_THREADS) k_bulk_rowcta(const Lattice* _
 
 // ---------------------------------------------------------------------------
 //  k_bulk_staged<S, PAR, MACRO, NST>: the rows away from walls, like
-//  k_bulk_batch, with the populations staged through shared memory.
+//  k_bulk_batch, with every row's populations staged in shared memory by bulk
+//  asynchronous copies and a producer warp that runs ahead of the consumers.
 //
 //  CTA c owns the contiguous rows [bounds[c], bounds[c+1]) of the row list
-//  (balanced by node count on the host) and walks them in order through NST
-//  stages. A stage holds the 19 direction-rows one row reads: for an even
-//  step A[i] of the row itself, for an odd step A[opp(i)] of the row
-//  (y - cy_i, z - cz_i), each a whole x-row. Thread 0 fills a stage with 19
-//  bulk asynchronous copies (cp.async.bulk, global -> shared, no multicast)
-//  that complete on the stage's mbarrier; the copy of each direction-row
-//  starts at the 16-byte boundary below it and is rounded up to 16 bytes, so
-//  it may read up to 15 bytes either side of the row (inside the population
-//  allocation, whose size is a multiple of 256 bytes). While a row is updated
-//  from its stage, the next NST - 1 rows are in flight, so the bytes in
-//  flight per SM sit in shared memory rather than in registers.
-//  Results are stored straight to global memory. Row partial sums are formed
-//  as in k_bulk_batch (bit-identical to a lattice run alone).
-//  Waits are bounded: a stage that does not arrive sets ST_WATCHDOG in the
-//  member's status word and the CTA stops.
+//  (balanced by node count on the host). A stage holds what one row reads:
+//  the 19 direction-rows (an even step reads A[i] of the row itself, an odd
+//  step A[opp(i)] of the row (y - cy_i, z - cz_i); each a whole x-row) and
+//  the row's flag bytes.
+//    warp 0 (producer)   for each row: wait until its stage is free (empty
+//                        barrier), copy the member's records into a member
+//                        slot if the member changed, and fill the stage with
+//                        20 cp.async.bulk copies (global -> shared, no
+//                        multicast) that complete on the stage's full barrier.
+//                        Each copy starts at the 16-byte boundary below its
+//                        row and is rounded up to 16 bytes, so it may read up
+//                        to 15 bytes either side of the row, always inside the
+//                        allocation (sizes are multiples of 256 bytes).
+//    warps 1-4 (update)  wait for the stage (full barrier), update the row's
+//                        nodes from it (stores go straight to global memory),
+//                        release the stage (empty barrier).
+//  NST - 1 rows are in flight while one is updated, so the bytes in flight per
+//  SM sit in shared memory rather than in registers. Row partial sums are
+//  formed as in k_bulk_batch (bit-identical to a lattice run alone).
+//  Every wait is bounded: on a timeout ST_WATCHDOG is set in the member's
+//  status word and the CTA stops. There is no CTA-wide barrier after the
+//  start, so a stopped warp cannot leave the others waiting unboundedly.
 // ---------------------------------------------------------------------------
-constexpr int STAGED_THREADS = 128;
+constexpr int STAGED_UPDATE_WARPS = 4;
+constexpr int STAGED_THREADS = 32 * (1 + STAGED_UPDATE_WARPS);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -196,6 +205,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* m, unsigned count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* m, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* m) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
 }
 // true once the phase with the given parity has completed; false after the
 // iteration limit (each try_wait also suspends for a while in hardware)
@@ -216,6 +228,28 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m))
                  : "memory");
+}
+// 16-byte aligned start and rounded-up length of the copy of [p, p + bytes)
+__device__ __forceinline__ void span16(const void* p, size_t bytes, uintptr_t& start, unsigned& len, int& off) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    start = a & ~(uintptr_t)15;
+    off = (int)(a - start);
+    len = (unsigned)((a + bytes - start + 15) & ~(uintptr_t)15);
+}
+
+// velocity set by a runtime index (lanes of the producer take one direction each)
+__device__ __forceinline__ int c_opp_rt(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+__device__ __forceinline__ int c_cy_rt(int i) {
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) if (k == i) v = CY(k);
+    return v;
+}
+__device__ __forceinline__ int c_cz_rt(int i) {
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) if (k == i) v = CZ(k);
+    return v;
 }
 
 // populations of node x from a stage (see update_node's Src parameter)
@@ -238,125 +272,164 @@ struct StagedSrc {
     }
 };
 
-template <class S, int PAR>
-__device__ __forceinline__ void stage_issue(typename S::T* sb, uint64_t* mbar, int* off, const Lattice& L,
-                                            const StreamArgs& a, int y, int z, int cap) {
-    using T = typename S::T;
-    const T* f = static_cast<const T*>(a.f);
-    uintptr_t start[Q];
-    unsigned bytes[Q], total = 0;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        int ys = y, zs = z, arr = i;
-        if (PAR == 1) {
-            arr = OPP(i);
-            ys = y - CY(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
-            zs = z - CZ(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
-        }
-        const uintptr_t src = reinterpret_cast<uintptr_t>(f + (size_t)arr * L.N + (size_t)L.nx * (ys + (size_t)L.ny * zs));
-        start[i] = src & ~(uintptr_t)15;
-        off[i] = (int)((src - start[i]) / sizeof(T));
-        bytes[i] = (unsigned)(((src + (uintptr_t)L.nx * sizeof(T) - start[i]) + 15) & ~(uintptr_t)15);
-        total += bytes[i];
-    }
-    mbar_expect_tx(mbar, total);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) bulk_g2s(sb + (size_t)i * cap, reinterpret_cast<const void*>(start[i]), bytes[i], mbar);
-}
-
 template <class S, int PAR, bool MACRO, int NST>
 __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* __restrict__ lat,
                                                                 const StreamArgs* __restrict__ args,
                                                                 const RowRef* __restrict__ rows,
                                                                 const int* __restrict__ bounds,
-                                                                double* __restrict__ row_part, BatchStep st, int cap) {
+                                                                double* __restrict__ row_part, BatchStep st, int cap,
+                                                                int fcap) {
     using T = typename S::T;
+    constexpr int MS = NST + 1;   // member slots: a slot is reused NST + 1 member changes later
     extern __shared__ __align__(128) unsigned char staged_raw[];
-    T* const buf = reinterpret_cast<T*>(staged_raw);
-    __shared__ __align__(8) uint64_t mbar[NST];
-    __shared__ Lattice sL[NST];
-    __shared__ StreamArgs sA[NST];
-    __shared__ ZoneBox sZ[NST];
-    __shared__ int sY[NST], sZc[NST], sP[NST], sOff[NST][Q];
-    __shared__ double red[2][BATCH_CHUNKS][4];
-    __shared__ int s_abort;
-    const int tid = threadIdx.x, lane = tid & 31;
+    T* const buf = reinterpret_cast<T*>(staged_raw);                                   // NST x Q x cap
+    uint8_t* const fbuf = staged_raw + (size_t)NST * Q * cap * sizeof(T);             // NST x fcap
+    __shared__ __align__(8) uint64_t full[NST], empty[NST];
+    __shared__ __align__(16) Lattice recL[MS];
+    __shared__ __align__(16) StreamArgs recA[MS];
+    __shared__ ZoneBox recZ[MS];
+    __shared__ int sSlot[NST], sY[NST], sZc[NST], sP[NST], sOff[NST][Q], sFoff[NST];
+    __shared__ double red[NST][BATCH_CHUNKS][4];   // chunk sums of the row in stage q
+    __shared__ int cnt[NST];                        // update warps done with the row in stage q
+    __shared__ volatile int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int r0 = bounds[blockIdx.x], r1 = bounds[blockIdx.x + 1];
     const bool sums_on = st.do_mass || MACRO;
 
-    auto issue = [&](int r, int s) {   // thread 0 only
-        const RowRef rr = rows[r];
-        sL[s] = lat[rr.m];
-        StreamArgs a = args[rr.m];
-        a.zslot = st.zslot; a.do_mass = st.do_mass; a.apply_corr = st.apply_corr;
-        sA[s] = a;
-        sZ[s] = a.sq->zone[st.zslot];
-        sY[s] = rr.y; sZc[s] = rr.z; sP[s] = rr.part;
-        stage_issue<S, PAR>(buf + (size_t)s * Q * cap, &mbar[s], sOff[s], sL[s], a, rr.y, rr.z, cap);
-    };
-
     if (tid == 0) {
-        for (int s = 0; s < NST; ++s) mbar_init(&mbar[s], 1);
+        for (int q = 0; q < NST; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], STAGED_UPDATE_WARPS);
+            cnt[q] = 0;
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
     }
     __syncthreads();
-    if (tid == 0)
-        for (int k = 0; k < NST && r0 + k < r1; ++k) issue(r0 + k, k);
 
-    uint32_t parity = 0;   // bit s: parity of the next phase of stage s
-    for (int r = r0, k = 0; r < r1; ++r, ++k) {
-        const int s = k % NST;
-        const bool ok = mbar_wait(&mbar[s], (parity >> s) & 1u);
-        parity ^= 1u << s;
-        if (!ok) {
-            s_abort = 1;
-        } else {
-            const Lattice& L = sL[s];
-            const StreamArgs& a = sA[s];
-            const int y = sY[s], z = sZc[s];
-            const T* sb = buf + (size_t)s * Q * cap;
-            const int nxr = (L.nx + 31) & ~31;
-            for (int x = tid; x < nxr; x += STAGED_THREADS) {
-                NodeSums sums;
-                if (x < L.nx) {
-                    const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
-                    const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[s], x, y, z);
-                    if (active)
-                        update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, 0, MACRO, sums,
-                                                          StagedSrc<T>{sb, sOff[s], cap, x, L.nx});
-                }
-                if (sums_on) {
-                    chunk_reduce(sums);
-                    if (lane == 0) {
-                        double* c = red[k & 1][x >> 5];
-                        c[0] = sums.fw[0]; c[1] = sums.fw[1]; c[2] = sums.fw[2]; c[3] = sums.mass;
-                    }
-                }
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        int last_m = -1, slot = -1;
+        RowRef batch{};   // lane j holds rows[base + j]: one load per 32 rows
+        for (int k = 0; r0 + k < r1; ++k) {
+            const int q = k % NST;
+            if ((k & 31) == 0 && r0 + k + lane < r1) batch = rows[r0 + k + lane];
+            if (k >= NST) {
+                int go = 1;   // decided by lane 0 for the whole warp
+                if (lane == 0) go = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1)) && !s_abort;
+                go = __shfl_sync(0xffffffffu, go, 0);
+                if (!go) { if (lane == 0) s_abort = 1; break; }
             }
-        }
-        __syncthreads();   // stage s and the records of row r are no longer read
-        if (s_abort) {
-            if (tid == 0) {
-                atomicOr(&sA[s].sq->status, ST_WATCHDOG);
-                for (int q = 0; q < NST; ++q) mbar_wait(&mbar[q], (parity >> q) & 1u);   // bounded
+            const int src_lane = k & 31;
+            const RowRef rr{__shfl_sync(0xffffffffu, batch.m, src_lane), __shfl_sync(0xffffffffu, batch.y, src_lane),
+                            __shfl_sync(0xffffffffu, batch.z, src_lane), __shfl_sync(0xffffffffu, batch.part, src_lane)};
+            if (rr.m != last_m) {
+                slot = (slot + 1) % MS;
+                const uint32_t* srcl = reinterpret_cast<const uint32_t*>(lat + rr.m);
+                uint32_t* dstl = reinterpret_cast<uint32_t*>(&recL[slot]);
+                for (int w = lane; w < (int)(sizeof(Lattice) / 4); w += 32) dstl[w] = srcl[w];
+                const uint32_t* srca = reinterpret_cast<const uint32_t*>(args + rr.m);
+                uint32_t* dsta = reinterpret_cast<uint32_t*>(&recA[slot]);
+                for (int w = lane; w < (int)(sizeof(StreamArgs) / 4); w += 32) dsta[w] = srca[w];
+                if (lane == 0) recZ[slot] = args[rr.m].sq->zone[st.zslot];
+                __syncwarp();
+                if (lane == 0) {
+                    recA[slot].zslot = st.zslot; recA[slot].do_mass = st.do_mass; recA[slot].apply_corr = st.apply_corr;
+                }
+                last_m = rr.m;
+                __syncwarp();
             }
-            return;
+            // lane i < Q copies direction-row i, lane Q the flag row
+            const Lattice& L = recL[slot];
+            uintptr_t start = 0;
+            unsigned len = 0;
+            int ob = 0;
+            if (lane < Q) {
+                const int i = lane;
+                int ys = rr.y, zs = rr.z, arr = i;
+                if (PAR == 1) {
+                    arr = c_opp_rt(i);
+                    ys = rr.y - c_cy_rt(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
+                    zs = rr.z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
+                }
+                const T* f = static_cast<const T*>(recA[slot].f);
+                span16(f + (size_t)arr * L.N + (size_t)L.nx * (ys + (size_t)L.ny * zs), (size_t)L.nx * sizeof(T), start,
+                       len, ob);
+                sOff[q][i] = ob / (int)sizeof(T);
+            } else if (lane == Q) {
+                span16(recA[slot].flag + (size_t)L.nx * (rr.y + (size_t)L.ny * rr.z), (size_t)L.nx, start, len, ob);
+                sFoff[q] = ob;
+            }
+            unsigned total = len;
+            for (int o = 16; o > 0; o >>= 1) total += __shfl_down_sync(0xffffffffu, total, o);
+            if (lane == 0) {
+                sSlot[q] = slot; sY[q] = rr.y; sZc[q] = rr.z; sP[q] = rr.part;
+                mbar_expect_tx(&full[q], total);   // releases the records written above
+            }
+            __syncwarp();
+            if (lane < Q)
+                bulk_g2s(buf + ((size_t)q * Q + lane) * cap, reinterpret_cast<const void*>(start), len, &full[q]);
+            else if (lane == Q)
+                bulk_g2s(fbuf + (size_t)q * fcap, reinterpret_cast<const void*>(start), len, &full[q]);
+            __syncwarp();
         }
-        if (tid == 0) {
+        return;
+    }
+
+    // ---------------- update warps ----------------
+    const int ut = tid - 32;   // 0 .. 32 * STAGED_UPDATE_WARPS - 1
+    for (int k = 0; r0 + k < r1; ++k) {
+        const int q = k % NST;
+        int go = 1;   // decided by lane 0 for the whole warp
+        if (lane == 0) {
+            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+            if (!ok && !s_abort) { s_abort = 1; atomicOr(&recA[sSlot[q]].sq->status, ST_WATCHDOG); }
+            go = ok && !s_abort;
+        }
+        go = __shfl_sync(0xffffffffu, go, 0);
+        if (!go) break;
+        const int slot = sSlot[q];
+        const Lattice& L = recL[slot];
+        const StreamArgs& a = recA[slot];
+        const int y = sY[q], z = sZc[q];
+        const T* sb = buf + (size_t)q * Q * cap;
+        const uint8_t* sf = fbuf + (size_t)q * fcap + sFoff[q];
+        const int nxr = (L.nx + 31) & ~31;
+        for (int x = ut; x < nxr; x += 32 * STAGED_UPDATE_WARPS) {
+            NodeSums sums;
+            if (x < L.nx) {
+                const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+                const bool active = (sf[x] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, recZ[slot], x, y, z);
+                if (active)
+                    update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, 0, MACRO, sums,
+                                                      StagedSrc<T>{sb, sOff[q], cap, x, L.nx});
+            }
             if (sums_on) {
-                const int nch = (sL[s].nx + 31) >> 5;
-                double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-                for (int c = 0; c < nch; ++c) {
-                    t0 += red[k & 1][c][0]; t1 += red[k & 1][c][1]; t2 += red[k & 1][c][2]; t3 += red[k & 1][c][3];
+                chunk_reduce(sums);
+                if (lane == 0) {
+                    double* c = red[q][x >> 5];
+                    c[0] = sums.fw[0]; c[1] = sums.fw[1]; c[2] = sums.fw[2]; c[3] = sums.mass;
                 }
-                double* out = row_part + (size_t)sP[s] * BLOCK_PART;
-                out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3;
             }
-            if (r + NST < r1) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(r + NST, s);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            if (sums_on) {
+                // the last update warp to finish the row adds its chunk sums in order
+                __threadfence_block();
+                if (atomicAdd(&cnt[q], 1) == STAGED_UPDATE_WARPS - 1) {
+                    __threadfence_block();
+                    const int nch = nxr >> 5;
+                    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+                    for (int c = 0; c < nch; ++c) {
+                        t0 += red[q][c][0]; t1 += red[q][c][1]; t2 += red[q][c][2]; t3 += red[q][c][3];
+                    }
+                    double* out = row_part + (size_t)sP[q] * BLOCK_PART;
+                    out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3;
+                    cnt[q] = 0;
+                }
             }
+            mbar_arrive(&empty[q]);   // the stage (and red[q]) may be refilled
         }
     }
 }

@@ -36,6 +36,7 @@ struct BatchArgs {
     const MemberParts* parts;
     const int* bounds;                 // staged kernel: row range of each CTA (grid + 1 entries)
     int cap;                           // staged kernel: elements per staged direction-row
+    int fcap;                          // staged kernel: bytes per staged flag row
 };
 
 struct Launchers {

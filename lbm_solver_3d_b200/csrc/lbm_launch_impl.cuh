@@ -116,25 +116,25 @@ static void batch_rowcta_launch(int par, bool macro, const BatchArgs& b, BatchSt
 
 template <class S, int PAR, bool MACRO, int NST>
 static void staged_one(int grid, const BatchArgs& b, BatchStep st, cudaStream_t s) {
-    const size_t smem = (size_t)NST * Q * b.cap * sizeof(typename S::T);
+    const size_t smem = (size_t)NST * ((size_t)Q * b.cap * sizeof(typename S::T) + b.fcap);
     k_bulk_staged<S, PAR, MACRO, NST><<<grid, STAGED_THREADS, smem, s>>>(b.lat, b.args, b.rows, b.bounds, b.row_part,
-                                                                        st, b.cap);
+                                                                        st, b.cap, b.fcap);
 }
 
 template <class S>
 static void batch_staged_launch(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st,
                                 cudaStream_t s) {
     if (b.nrows == 0) return;
-    const int sel = (par ? 4 : 0) | (macro ? 2 : 0) | (nst == 3 ? 1 : 0);
+    const int sel = (par ? 4 : 0) | (macro ? 2 : 0) | (nst == 4 ? 1 : 0);
     switch (sel) {
-        case 0: staged_one<S, 0, false, 2>(grid, b, st, s); break;
-        case 1: staged_one<S, 0, false, 3>(grid, b, st, s); break;
-        case 2: staged_one<S, 0, true, 2>(grid, b, st, s); break;
-        case 3: staged_one<S, 0, true, 3>(grid, b, st, s); break;
-        case 4: staged_one<S, 1, false, 2>(grid, b, st, s); break;
-        case 5: staged_one<S, 1, false, 3>(grid, b, st, s); break;
-        case 6: staged_one<S, 1, true, 2>(grid, b, st, s); break;
-        default: staged_one<S, 1, true, 3>(grid, b, st, s); break;
+        case 0: staged_one<S, 0, false, 3>(grid, b, st, s); break;
+        case 1: staged_one<S, 0, false, 4>(grid, b, st, s); break;
+        case 2: staged_one<S, 0, true, 3>(grid, b, st, s); break;
+        case 3: staged_one<S, 0, true, 4>(grid, b, st, s); break;
+        case 4: staged_one<S, 1, false, 3>(grid, b, st, s); break;
+        case 5: staged_one<S, 1, false, 4>(grid, b, st, s); break;
+        case 6: staged_one<S, 1, true, 3>(grid, b, st, s); break;
+        default: staged_one<S, 1, true, 4>(grid, b, st, s); break;
     }
 }
 
@@ -166,9 +166,9 @@ static cudaError_t prepare_launch() {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
     if (e != cudaSuccess) return e;
-    cudaError_t es[8] = {staged_attr<S, 0, false, 2>(), staged_attr<S, 0, false, 3>(), staged_attr<S, 0, true, 2>(),
-                         staged_attr<S, 0, true, 3>(),  staged_attr<S, 1, false, 2>(), staged_attr<S, 1, false, 3>(),
-                         staged_attr<S, 1, true, 2>(),  staged_attr<S, 1, true, 3>()};
+    cudaError_t es[8] = {staged_attr<S, 0, false, 3>(), staged_attr<S, 0, false, 4>(), staged_attr<S, 0, true, 3>(),
+                         staged_attr<S, 0, true, 4>(),  staged_attr<S, 1, false, 3>(), staged_attr<S, 1, false, 4>(),
+                         staged_attr<S, 1, true, 3>(),  staged_attr<S, 1, true, 4>()};
     for (cudaError_t x : es)
         if (x != cudaSuccess) return x;
     return cudaSuccess;

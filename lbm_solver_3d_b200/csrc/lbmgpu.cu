@@ -1099,7 +1099,7 @@ struct lbmgpu_batch {
     // tiling of the bulk launch (autotuned): tile > 0 is k_bulk_batch with that
     // many threads per row, tile < 0 is k_bulk_staged with -tile stages;
     // the grid is bps CTAs per SM
-    int tile = 32, bps = 4;
+    int tile = LBMGPU_TILE_ROWCTA, bps = 4;
     int* d_bounds = nullptr;       // staged kernel: row range of each CTA
     int bounds_cap = 0, bounds_grid = 0;
     std::vector<long long> row_prefix;   // nodes in the rows before row r (rows away from walls)
@@ -1402,6 +1402,7 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
         for (int i = 0; i < n; ++i) nxmax = std::max(nxmax, ps[i].nx);
         const size_t es = b->lz->esize;
         b->ba.cap = (int)(((size_t)nxmax * es + 32 + 15) / 16 * 16 / es);
+        b->ba.fcap = (nxmax + 32 + 15) / 16 * 16;
         b->row_prefix.assign(rows.size() + 1, 0);
         for (size_t r = 0; r < rows.size(); ++r) b->row_prefix[r + 1] = b->row_prefix[r] + ps[rows[r].m].nx;
     }
@@ -1480,11 +1481,11 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
 
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (!b) return LBMGPU_ERR_INVALID;
-    if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED2 && tile != LBMGPU_TILE_STAGED3 &&
+    if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED3 && tile != LBMGPU_TILE_STAGED4 &&
          tile != LBMGPU_TILE_ROWCTA) ||
         ctas_per_sm < 1 || ctas_per_sm > 16)
         return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA or "
-                                            "LBMGPU_TILE_STAGED2/3, and ctas_per_sm 1..16");
+                                            "LBMGPU_TILE_STAGED3/4, and ctas_per_sm 1..16");
     BTRY(b, cudaSetDevice(b->p0.device));
     BTRY(b, cudaStreamSynchronize(b->sa));
     BTRY(b, cudaStreamSynchronize(b->sb));
@@ -1513,7 +1514,7 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaEvent_t e0, e1;
     BTRY(b, cudaEventCreate(&e0));
     BTRY(b, cudaEventCreate(&e1));
-    const int tiles[6] = {LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED2, LBMGPU_TILE_STAGED3};
+    const int tiles[6] = {LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4};
     const int bpss[7] = {1, 2, 3, 4, 5, 6, 8};
     double best = 1e30;
     int btx = b->tile, bbps = b->bps;
