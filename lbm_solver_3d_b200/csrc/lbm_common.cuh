@@ -99,7 +99,15 @@ struct ZoneBox {
     int lo[3], w[3];
 };
 constexpr int ZONE_SLOTS = 3;
-constexpr int ZONE_MARGIN = 4;  // cells around the remap box (see k_squirmer.cuh)
+// Cells around the remap box. The zone of step s + 2 is laid out around the
+// box of the position after step s; it must hold (a) every node whose flags
+// the squirmer update after step s + 1 changes (inside the box of the next
+// position) and (b) every node whose density that update's refill reads
+// (inside that box too), whose densities the zone kernel of step s + 1 stored
+// from the zone laid out one step earlier. The centre moves less than one cell
+// per step (checked: ST_REMAP_RANGE), so across two steps each box bound
+// shifts by at most 2 cells.
+constexpr int ZONE_MARGIN = 2;
 
 // Zone width along an axis: the remap box (lbm.cpp:273-275) is at most
 // 2*ceil(R) + 6 cells wide; the zone adds ZONE_MARGIN cells on each side.
