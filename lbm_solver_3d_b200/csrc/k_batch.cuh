@@ -104,7 +104,8 @@ __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-//  k_bulk_rowcta<S, PAR, MACRO>: the rows away from walls, one CTA of
+//  k_bulk_rowcta<S, PAR, MACRO, WR>: the rows away from walls (WR: the rows
+//  next to a wall, with their bounce-back and wall momentum), one CTA of
 //  ROWCTA_THREADS threads per row (grid = rows; the hardware scheduler keeps
 //  the SMs full, as for k_bulk on a single lattice). Warp 0 copies the row's
 //  member records into shared memory; nodes x = tid, tid + ROWCTA_THREADS.
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ 
 // ---------------------------------------------------------------------------
 constexpr int ROWCTA_THREADS = 128;
 
-template <class S, int PAR, bool MACRO>
+template <class S, int PAR, bool MACRO, bool WR>
 __global__ void __launch_bounds__(ROWCTA_THREADS) k_bulk_rowcta(const Lattice* __restrict__ lat,
                                                                 const StreamArgs* __restrict__ args,
                                                                 const RowRef* __restrict__ rows,
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(ROWCTA_THREADS) k_bulk_rowcta(const Lattice* _
         if (x < L.nx) {
             const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
             const bool active = (sA.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ, x, y, z);
-            if (active) update_node<S, PAR, false, MACRO>(L, sA, n, x, y, z, 0, 0, MACRO, sums);
+            if (active) update_node<S, PAR, false, MACRO>(L, sA, n, x, y, z, 0, WR ? wall_row(L, y, z) : (uint8_t)0, MACRO, sums);
         }
         if (sums_on) {
             chunk_reduce(sums);

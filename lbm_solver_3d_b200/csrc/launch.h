@@ -64,8 +64,8 @@ struct Launchers {
     void (*batch_zone)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
     // the rows away from walls through shared-memory stages (k_bulk_staged)
     void (*batch_staged)(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
-    // the rows away from walls, one CTA per row (k_bulk_rowcta)
-    void (*batch_rowcta)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    // one CTA per row (k_bulk_rowcta): rows away from walls, or next to one
+    void (*batch_rowcta)(int par, bool macro, bool wallrows, const BatchArgs& b, BatchStep st, cudaStream_t s);
     size_t esize;
     void (*batch_squirmer)(const BatchArgs& b, SqStep st, cudaStream_t s);
 };

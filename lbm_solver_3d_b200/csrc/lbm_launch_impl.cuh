@@ -103,14 +103,24 @@ static void batch_bulk_launch(int par, bool macro, bool wr, int tx, int grid, co
     }
 }
 
+template <class S, int PAR, bool MACRO, bool WR>
+static void rowcta_one(const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    const RowRef* rows = WR ? b.wrows : b.rows;
+    const int n = WR ? b.nwrows : b.nrows;
+    if (n) k_bulk_rowcta<S, PAR, MACRO, WR><<<n, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, rows, b.row_part, st);
+}
+
 template <class S>
-static void batch_rowcta_launch(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s) {
-    if (b.nrows == 0) return;
-    switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
-        case 0: k_bulk_rowcta<S, 0, false><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
-        case 1: k_bulk_rowcta<S, 0, true><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
-        case 2: k_bulk_rowcta<S, 1, false><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
-        default: k_bulk_rowcta<S, 1, true><<<b.nrows, ROWCTA_THREADS, 0, s>>>(b.lat, b.args, b.rows, b.row_part, st); break;
+static void batch_rowcta_launch(int par, bool macro, bool wr, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    switch ((par ? 4 : 0) | (macro ? 2 : 0) | (wr ? 1 : 0)) {
+        case 0: rowcta_one<S, 0, false, false>(b, st, s); break;
+        case 1: rowcta_one<S, 0, false, true>(b, st, s); break;
+        case 2: rowcta_one<S, 0, true, false>(b, st, s); break;
+        case 3: rowcta_one<S, 0, true, true>(b, st, s); break;
+        case 4: rowcta_one<S, 1, false, false>(b, st, s); break;
+        case 5: rowcta_one<S, 1, false, true>(b, st, s); break;
+        case 6: rowcta_one<S, 1, true, false>(b, st, s); break;
+        default: rowcta_one<S, 1, true, true>(b, st, s); break;
     }
 }
 

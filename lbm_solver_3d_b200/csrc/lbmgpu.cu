@@ -1177,7 +1177,7 @@ int set_bounds(lbmgpu_batch* b, int grid) {
 // the bulk launch (rows away from walls) with a given tiling
 void launch_bulk(lbmgpu_batch* b, int tile, int grid, int par, bool macro, BatchStep bst, cudaStream_t s) {
     if (tile < 0) b->lz->batch_staged(par, macro, -tile, grid, b->ba, bst, s);
-    else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, false, b->ba, bst, s);
     else b->lz->batch_bulk(par, macro, false, tile, grid, b->ba, bst, s);
 }
 
@@ -1194,8 +1194,7 @@ void issue_batch(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb, long long s,
     cudaStreamWaitEvent(sb, b->ev_b[(s - 1) & 1], 0);
     int k = 1;
     if (b->ba.nwrows) {
-        const int wgrid = std::max(1, std::min(grid, (b->ba.nwrows + 7) / 8));
-        b->lz->batch_bulk(par, macro, true, 32, wgrid, b->ba, bst, sb);
+        b->lz->batch_rowcta(par, macro, true, b->ba, bst, sb);   // one CTA per wall row
         ++k;
     }
     if (b->has_sq) { b->lz->batch_zone(par, macro, b->ba, bst, sb); ++k; }
