@@ -190,13 +190,16 @@ def workload_config(args, p, reference=False):
 
 
 def bench_ensemble(args):
-    """Trajectories per hour: the 256-member slit-channel ensemble (FP32-shifted,
-    30000 steps per trajectory, autotuned bulk tiling, CUDA graphs) against the
-    same members solved one after another with the plain FP64 path (and with
-    FP32 alone, for reference). The sequential time per step is measured on a
-    seeded sample of members, each alone, and scaled to all 256."""
+    """Trajectories per hour: the 256-member slit-channel ensemble (FP32-shifted
+    unless --precision says otherwise, 30000 steps per trajectory, autotuned
+    bulk tiling, CUDA graphs) against the same members solved one after
+    another with the plain FP64 path (and with FP32 alone, for reference). The
+    sequential time per step is measured on a seeded sample of members, each
+    alone, and scaled to all 256. With N ranks the members are split across
+    the GPUs (shard_members, no exchange): weak in the per-GPU work, and the
+    whole ensemble's step time is the slowest rank's."""
     import torch
-    from lbm_solver_3d_b200.ensemble import Ensemble
+    from lbm_solver_3d_b200.ensemble import Ensemble, shard_members
     from lbm_solver_3d_b200.solver import Solver
     from lbm_solver_3d_b200.workloads import ensemble_members
 
@@ -207,7 +210,18 @@ def bench_ensemble(args):
                               "process; its ensemble is the sequential loop measured by --workload ensemble"}))
         return
     torch.cuda.set_device(local)
-    ps = ensemble_members(256)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    all_ps = ensemble_members(256)
+    prec = args.precision if args.precision_set else "fp32"
+    for p in all_ps:
+        p.update(precision=prec, device=local)
+    mine = shard_members(all_ps, rank, world)
+    ps = [all_ps[i] for i in mine]
     traj_steps = ps[0].steps
     stream = torch.cuda.Stream(device=local)
     ens = Ensemble(ps)
@@ -217,6 +231,9 @@ def bench_ensemble(args):
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = ens.launch_count()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.start()
         with torch.cuda.stream(stream):
@@ -225,56 +242,70 @@ def bench_ensemble(args):
             ev1.record(stream)
         torch.cuda.synchronize()
         clk.stop()
-    ms_step = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        pg.barrier()
+    t_max = torch.tensor([ev0.elapsed_time(ev1) / args.steps], device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t_max, op=pg.ReduceOp.MAX)
+    ms_step = float(t_max.item())
     launches = ens.launch_count() - l0
     bulk_ms = ens.time_bulk(reps=5)
     cells = ens.cells
     ens.close()
-    traj_h = len(ps) * 3600.0 / (traj_steps * ms_step * 1e-3)
+    traj_h = len(all_ps) * 3600.0 / (traj_steps * ms_step * 1e-3)
 
-    # sequential solves of a seeded sample of members, each alone
-    rng = np.random.default_rng(7)
-    sample = sorted(rng.choice(len(ps), size=12, replace=False).tolist())
-    seq = {}
-    for prec in ("fp64", "fp32"):
-        per = []
-        for i in sample:
-            q = ps[i].copy().update(precision=prec)
-            s = Solver(q)
-            s.set_stream(stream.cuda_stream)
-            s.run(args.warmup)
-            torch.cuda.synchronize()
-            with torch.cuda.stream(stream):
-                ev0.record(stream)
-                s.run(args.steps)
-                ev1.record(stream)
-            torch.cuda.synchronize()
-            per.append(ev0.elapsed_time(ev1) / args.steps)
-            s.close()
-        mean_ms = float(np.mean(per))
-        seq[prec] = {"ms_per_step_mean": mean_ms, "trajectories_per_hour": 3600.0 / (traj_steps * mean_ms * 1e-3)}
+    seq = None
+    if rank == 0:
+        # sequential solves of a seeded sample of members, each alone
+        rng = np.random.default_rng(7)
+        sample = sorted(rng.choice(len(all_ps), size=12, replace=False).tolist())
+        seq = {"sample_members": sample}
+        for sp in ("fp64", "fp32"):
+            per = []
+            for i in sample:
+                q = all_ps[i].copy().update(precision=sp)
+                s = Solver(q)
+                s.set_stream(stream.cuda_stream)
+                s.run(args.warmup)
+                torch.cuda.synchronize()
+                with torch.cuda.stream(stream):
+                    ev0.record(stream)
+                    s.run(args.steps)
+                    ev1.record(stream)
+                torch.cuda.synchronize()
+                per.append(ev0.elapsed_time(ev1) / args.steps)
+                s.close()
+            mean_ms = float(np.mean(per))
+            seq[sp] = {"ms_per_step_mean": mean_ms,
+                       "trajectories_per_hour": 3600.0 / (traj_steps * mean_ms * 1e-3)}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
     peak, peak_kind = peaks()
-    bytes_step = 2 * 19 * 4 * cells
+    bytes_step = 2 * 19 * BYTES[prec] * cells
     line = {
         "metric": "ensemble trajectories/hour (256 slit channels, 30000 steps each)",
-        "value": traj_h, "unit": "trajectories/h", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "value": traj_h, "unit": "trajectories/h", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32-shifted", "data": "synthetic",
+        "dtype": DTYPE[prec], "data": "synthetic",
         "config": {"workload": "ensemble: 256 slit-channel squirmers, Nx 64-160, Ny/Nz 48-96, a 4-8, "
-                               "beta -5..5, angle -30..30 deg, seed 2024", "cells": cells,
-                   "tiling": tune, "l2": "populations larger than L2; no flush"},
-        "sequential": {"sample_members": sample, **seq},
+                               "beta -5..5, angle -30..30 deg, seed 2024",
+                   "members_on_rank0": len(ps), "cells_on_rank0": cells, "tiling_rank0": tune,
+                   "parallelism": f"members split across {world} GPU(s)",
+                   "l2": "populations larger than L2; no flush"},
+        "sequential": seq,
         "speedup_vs_sequential_fp64": traj_h / seq["fp64"]["trajectories_per_hour"],
         "speedup_vs_sequential_fp32": traj_h / seq["fp32"]["trajectories_per_hour"],
-        "roofline": {"bound": "hbm", "kernel": "k_bulk_batch", "launch_ms": bulk_ms,
+        "roofline": {"bound": "hbm", "kernel": "ensemble bulk kernel (rank 0)", "launch_ms": bulk_ms,
                      "achieved": bytes_step / (bulk_ms * 1e-3) / 1e9, "peak": peak,
                      "frac": bytes_step / (bulk_ms * 1e-3) / 1e9 / peak, "unit": "GB/s",
                      "peak_source": peak_kind, "step_frac": bytes_step / (ms_step * 1e-3) / 1e9 / peak},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -282,12 +313,15 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=100)
-    ap.add_argument("--precision", default="fp32", choices=list(BYTES))
+    ap.add_argument("--precision", default=None, choices=list(BYTES))
     ap.add_argument("--workload", default="bulk_0")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    args.precision_set = args.precision is not None
+    if args.precision is None:
+        args.precision = "fp32"
 
     if args.workload == "ensemble":
         bench_ensemble(args)

@@ -19,6 +19,23 @@ from .params import Params
 from .solver import Solver
 
 
+def shard_members(members: list[Params], rank: int, world: int) -> list[int]:
+    """Indices of the members that rank `rank` of `world` runs: the members are
+    independent, so a multi-GPU ensemble splits them across ranks with no
+    exchange. Largest first, each to the rank with the fewest nodes so far
+    (ties to the lower rank): every rank computes the same assignment."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    order = sorted(range(len(members)), key=lambda i: (-members[i].ncells, i))
+    load = [0] * world
+    owner = {}
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += members[i].ncells
+    return sorted(i for i in range(len(members)) if owner[i] == rank)
+
+
 class Ensemble:
     def __init__(self, members: list[Params], autotune: bool = False, tune_reps: int = 5):
         if not members:
