@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ 
 constexpr int ROWCTA_THREADS = 128;
 
 template <class S, int PAR, bool MACRO, bool WR>
-__global__ void __launch_bounds__(ROWCTA_THREADS) k_bulk_rowcta(const Lattice* __restrict__ lat,
+__global__ void __launch_bounds__(ROWCTA_THREADS, S::shifted ? 7 : 4) k_bulk_rowcta(const Lattice* __restrict__ lat,
                                                                 const StreamArgs* __restrict__ args,
                                                                 const RowRef* __restrict__ rows,
                                                                 double* __restrict__ row_part, BatchStep st) {
@@ -124,16 +124,18 @@ __global__ void __launch_bounds__(ROWCTA_THREADS) k_bulk_rowcta(const Lattice* _
     __shared__ double red[BATCH_CHUNKS][4];
     const int tid = threadIdx.x, lane = tid & 31;
     const RowRef rr = rows[blockIdx.x];   // uniform: one row per CTA
-    if (tid < 32) {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(lat + rr.m);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&sL);
-        for (int k = lane; k < (int)(sizeof(Lattice) / 4); k += 32) dst[k] = src[k];
-        const uint32_t* srca = reinterpret_cast<const uint32_t*>(args + rr.m);
-        uint32_t* dsta = reinterpret_cast<uint32_t*>(&sA);
-        for (int k = lane; k < (int)(sizeof(StreamArgs) / 4); k += 32) dsta[k] = srca[k];
-        if (lane == 0) sZ = args[rr.m].sq->zone[st.zslot];
-        __syncwarp();
-        if (lane == 0) { sA.zslot = st.zslot; sA.do_mass = st.do_mass; sA.apply_corr = st.apply_corr; }
+    {   // the member's records, one word per thread, with this step's settings
+        constexpr int NL = (int)(sizeof(Lattice) / 4), NA = (int)(sizeof(StreamArgs) / 4);
+        static_assert(NL <= ROWCTA_THREADS && NA <= ROWCTA_THREADS, "one word per thread");
+        if (tid < NL) reinterpret_cast<uint32_t*>(&sL)[tid] = reinterpret_cast<const uint32_t*>(lat + rr.m)[tid];
+        if (tid < NA) {
+            uint32_t w = reinterpret_cast<const uint32_t*>(args + rr.m)[tid];
+            if (tid == (int)(offsetof(StreamArgs, zslot) / 4)) w = (uint32_t)st.zslot;
+            if (tid == (int)(offsetof(StreamArgs, do_mass) / 4)) w = (uint32_t)st.do_mass;
+            if (tid == (int)(offsetof(StreamArgs, apply_corr) / 4)) w = (uint32_t)st.apply_corr;
+            reinterpret_cast<uint32_t*>(&sA)[tid] = w;
+        }
+        if (tid == ROWCTA_THREADS - 1) sZ = args[rr.m].sq->zone[st.zslot];
     }
     __syncthreads();
     const bool sums_on = st.do_mass || MACRO;
