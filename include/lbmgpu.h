@@ -294,12 +294,15 @@ int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
  *     x-row, loading populations straight from global memory;
  *   tile = LBMGPU_TILE_ROWCTA: one CTA of 128 threads per row (grid = rows,
  *     ctas_per_sm unused);
+ *   tile = LBMGPU_TILE_CHUNK: one warp per 32 consecutive nodes of a row
+ *     (grid = chunks / 4, ctas_per_sm unused);
  *   tile = LBMGPU_TILE_STAGED3 / _STAGED4: each CTA owns a contiguous range
  *     of rows (equal node counts); a producer warp stages every row's
  *     populations and flags in shared memory with bulk asynchronous copies,
  *     3 or 4 rows deep, while four warps update the rows already staged.
  * ctas_per_sm (1..16): the grid is that many CTAs per SM. */
 #define LBMGPU_TILE_ROWCTA 1
+#define LBMGPU_TILE_CHUNK 2
 #define LBMGPU_TILE_STAGED3 (-3)
 #define LBMGPU_TILE_STAGED4 (-4)
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm);

@@ -170,6 +170,79 @@ __global__ void __launch_bounds__(ROWCTA_THREADS, S::shifted ? 7 : 4) k_bulk_row
 }
 
 // ---------------------------------------------------------------------------
+//  k_bulk_chunk<S, PAR, MACRO>: the rows away from walls cut into chunks of 32
+//  consecutive nodes; every warp owns one chunk (4 warps per CTA, grid =
+//  chunks / 4) and runs on its own: it copies its member's records into its
+//  shared slot (one word per lane), with no CTA-wide barrier, and its lanes
+//  update x0 + lane. Lanes are idle only past the end of a row, in its last
+//  chunk. On steps that sum, each chunk's partial (the shuffle tree over its
+//  32 nodes) goes to chunk_part, and k_fold_chunks adds a row's chunks in
+//  order: the row partial is bit-identical to k_bulk's (0 + c0 + c1 + ...).
+// ---------------------------------------------------------------------------
+constexpr int CHUNK_WARPS = 4;
+
+template <class S, int PAR, bool MACRO>
+__global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_chunk(
+    const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args, const ChunkRef* __restrict__ chunks,
+    int nchunks, double* __restrict__ chunk_part, BatchStep st) {
+    __shared__ __align__(16) Lattice sL[CHUNK_WARPS];
+    __shared__ __align__(16) StreamArgs sA[CHUNK_WARPS];
+    __shared__ ZoneBox sZ[CHUNK_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * CHUNK_WARPS + w;
+    if (c >= nchunks) return;   // warp-uniform
+    const ChunkRef cr = chunks[c];
+    {
+        constexpr int NL = (int)(sizeof(Lattice) / 4), NA = (int)(sizeof(StreamArgs) / 4);
+        const uint32_t* srcl = reinterpret_cast<const uint32_t*>(lat + cr.m);
+        uint32_t* dstl = reinterpret_cast<uint32_t*>(&sL[w]);
+        for (int k = lane; k < NL; k += 32) dstl[k] = srcl[k];
+        const uint32_t* srca = reinterpret_cast<const uint32_t*>(args + cr.m);
+        uint32_t* dsta = reinterpret_cast<uint32_t*>(&sA[w]);
+        for (int k = lane; k < NA; k += 32) {
+            uint32_t v = srca[k];
+            if (k == (int)(offsetof(StreamArgs, zslot) / 4)) v = (uint32_t)st.zslot;
+            if (k == (int)(offsetof(StreamArgs, do_mass) / 4)) v = (uint32_t)st.do_mass;
+            if (k == (int)(offsetof(StreamArgs, apply_corr) / 4)) v = (uint32_t)st.apply_corr;
+            dsta[k] = v;
+        }
+        if (lane == 0) sZ[w] = args[cr.m].sq->zone[st.zslot];
+        __syncwarp();
+    }
+    const Lattice& L = sL[w];
+    const StreamArgs& a = sA[w];
+    NodeSums sums;
+    const int x = cr.x0 + lane;
+    if (x < L.nx) {
+        const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)cr.y + (unsigned)L.ny * (unsigned)cr.z);
+        const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, cr.y, cr.z);
+        if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, cr.y, cr.z, 0, 0, MACRO, sums);
+    }
+    if (st.do_mass || MACRO) {
+        chunk_reduce(sums);
+        if (lane == 0) {
+            double* o = chunk_part + (size_t)c * BLOCK_PART;
+            o[0] = sums.fw[0]; o[1] = sums.fw[1]; o[2] = sums.fw[2]; o[3] = sums.mass;
+        }
+    }
+}
+
+// row partial = its chunk partials added in order, from 0 (one thread per row)
+static __global__ void k_fold_chunks(const RowChunks* __restrict__ rc, int nrows, const double* __restrict__ chunk_part,
+                              double* __restrict__ row_part) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const RowChunks q = rc[r];
+    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    for (int k = 0; k < q.count; ++k) {
+        const double* p = chunk_part + (size_t)(q.first + k) * BLOCK_PART;
+        t0 += p[0]; t1 += p[1]; t2 += p[2]; t3 += p[3];
+    }
+    double* o = row_part + (size_t)q.part * BLOCK_PART;
+    o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+}
+
+// ---------------------------------------------------------------------------
 //  k_bulk_staged<S, PAR, MACRO, NST>: the rows away from walls, like
 //  k_bulk_batch, with every row's populations staged in shared memory by bulk
 //  asynchronous copies and a producer warp that runs ahead of the consumers.

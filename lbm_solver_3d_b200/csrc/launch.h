@@ -35,6 +35,9 @@ struct BatchArgs {
     int nmembers;
     const MemberParts* parts;
     const int* bounds;                 // staged kernel: row range of each CTA (grid + 1 entries)
+    const ChunkRef* chunks; int nchunks;   // chunk kernel: 32-node pieces of the rows away from walls
+    const RowChunks* rowchunks;        // chunk kernel: each row's chunks
+    double* chunk_part;                // chunk kernel: partial sums per chunk
     int cap;                           // staged kernel: elements per staged direction-row
     int fcap;                          // staged kernel: bytes per staged flag row
 };
@@ -64,6 +67,8 @@ struct Launchers {
     void (*batch_zone)(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s);
     // the rows away from walls through shared-memory stages (k_bulk_staged)
     void (*batch_staged)(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    // one warp per 32-node chunk (k_bulk_chunk, then k_fold_chunks when summing)
+    void (*batch_chunk)(int par, bool macro, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s);
     // one CTA per row (k_bulk_rowcta): rows away from walls, or next to one
     void (*batch_rowcta)(int par, bool macro, bool wallrows, const BatchArgs& b, BatchStep st, cudaStream_t s);
     size_t esize;

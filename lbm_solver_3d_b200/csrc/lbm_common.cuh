@@ -192,6 +192,12 @@ struct RowRef {
     int m, y, z;       // member, row coordinates
     int part;          // entry of the row's partial sums (member base + y + ny*z)
 };
+struct ChunkRef {      // 32 consecutive nodes [x0, x0 + 32) of one row (the last may be short)
+    int m, y, z, x0;
+};
+struct RowChunks {     // the chunks of one row, and where its partial sums go
+    int first, count, part, pad;
+};
 struct BatchStep {     // per-step settings shared by all members
     int zslot, do_mass, apply_corr;
 };

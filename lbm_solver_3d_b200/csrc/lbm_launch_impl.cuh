@@ -124,6 +124,24 @@ static void batch_rowcta_launch(int par, bool macro, bool wr, const BatchArgs& b
     }
 }
 
+template <class S, int PAR, bool MACRO>
+static void chunk_one(bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    if (b.nchunks == 0) return;
+    k_bulk_chunk<S, PAR, MACRO><<<(b.nchunks + CHUNK_WARPS - 1) / CHUNK_WARPS, 32 * CHUNK_WARPS, 0, s>>>(
+        b.lat, b.args, b.chunks, b.nchunks, b.chunk_part, st);
+    if (sums) k_fold_chunks<<<(b.nrows + 255) / 256, 256, 0, s>>>(b.rowchunks, b.nrows, b.chunk_part, b.row_part);
+}
+
+template <class S>
+static void batch_chunk_launch(int par, bool macro, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
+        case 0: chunk_one<S, 0, false>(sums, b, st, s); break;
+        case 1: chunk_one<S, 0, true>(sums, b, st, s); break;
+        case 2: chunk_one<S, 1, false>(sums, b, st, s); break;
+        default: chunk_one<S, 1, true>(sums, b, st, s); break;
+    }
+}
+
 template <class S, int PAR, bool MACRO, int NST>
 static void staged_one(int grid, const BatchArgs& b, BatchStep st, cudaStream_t s) {
     const size_t smem = (size_t)NST * ((size_t)Q * b.cap * sizeof(typename S::T) + b.fcap);
@@ -201,6 +219,7 @@ static Launchers make_launchers() {
     l.batch_squirmer = &batch_squirmer_launch<S>;
     l.batch_staged = &batch_staged_launch<S>;
     l.batch_rowcta = &batch_rowcta_launch<S>;
+    l.batch_chunk = &batch_chunk_launch<S>;
     l.esize = sizeof(typename S::T);
     return l;
 }

@@ -1099,8 +1099,11 @@ struct lbmgpu_batch {
     // tiling of the bulk launch (autotuned): tile > 0 is k_bulk_batch with that
     // many threads per row, tile < 0 is k_bulk_staged with -tile stages;
     // the grid is bps CTAs per SM
-    int tile = LBMGPU_TILE_ROWCTA, bps = 4;
+    int tile = LBMGPU_TILE_CHUNK, bps = 4;
     int* d_bounds = nullptr;       // staged kernel: row range of each CTA
+    ChunkRef* d_chunks = nullptr;  // chunk kernel
+    RowChunks* d_rowchunks = nullptr;
+    double* chunk_part = nullptr;
     int bounds_cap = 0, bounds_grid = 0;
     std::vector<long long> row_prefix;   // nodes in the rows before row r (rows away from walls)
     long long cells = 0, t = 0, launches = 0;
@@ -1134,7 +1137,8 @@ void batch_free(lbmgpu_batch* b) {
     }
     b->m.clear();
     void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts,
-                    b->row_part, b->zone_part, b->d_status, b->d_bounds};
+                    b->row_part, b->zone_part, b->d_status, b->d_bounds, b->d_chunks, b->d_rowchunks,
+                    b->chunk_part};
     for (void* q : ptrs) if (q) cudaFree(q);
     for (cudaEvent_t e : {b->ev_b[0], b->ev_b[1], b->ev_z, b->ev_s, b->ev_fork, b->ev_join})
         if (e) cudaEventDestroy(e);
@@ -1178,6 +1182,7 @@ int set_bounds(lbmgpu_batch* b, int grid) {
 void launch_bulk(lbmgpu_batch* b, int tile, int grid, int par, bool macro, BatchStep bst, cudaStream_t s) {
     if (tile < 0) b->lz->batch_staged(par, macro, -tile, grid, b->ba, bst, s);
     else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, false, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_CHUNK) b->lz->batch_chunk(par, macro, macro || bst.do_mass, b->ba, bst, s);
     else b->lz->batch_bulk(par, macro, false, tile, grid, b->ba, bst, s);
 }
 
@@ -1380,7 +1385,25 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
         sqa[i].block_part_w = nullptr;
         sqa[i].nblocks_w = 0;
     }
+    // 32-node chunks of the rows away from walls, and each row's chunk range
+    std::vector<ChunkRef> chunks;
+    std::vector<RowChunks> rowchunks(rows.size());
+    for (size_t r = 0; r < rows.size(); ++r) {
+        const int nx = ps[rows[r].m].nx;
+        rowchunks[r] = RowChunks{(int)chunks.size(), (nx + 31) / 32, rows[r].part, 0};
+        for (int x0 = 0; x0 < nx; x0 += 32) chunks.push_back(ChunkRef{rows[r].m, rows[r].y, rows[r].z, x0});
+    }
+    CB(cudaMalloc(&b->d_chunks, std::max<size_t>(1, chunks.size()) * sizeof(ChunkRef)));
+    CB(cudaMalloc(&b->d_rowchunks, std::max<size_t>(1, rowchunks.size()) * sizeof(RowChunks)));
+    CB(cudaMalloc(&b->chunk_part, std::max<size_t>(1, chunks.size()) * BLOCK_PART * sizeof(double)));
     cudaStream_t st = b->sa;
+    if (!chunks.empty()) {
+        CB(cudaMemcpyAsync(b->d_chunks, chunks.data(), chunks.size() * sizeof(ChunkRef), cudaMemcpyHostToDevice, st));
+        CB(cudaMemcpyAsync(b->d_rowchunks, rowchunks.data(), rowchunks.size() * sizeof(RowChunks),
+                           cudaMemcpyHostToDevice, st));
+    }
+    b->ba.chunks = b->d_chunks; b->ba.nchunks = (int)chunks.size();
+    b->ba.rowchunks = b->d_rowchunks; b->ba.chunk_part = b->chunk_part;
     CB(cudaMemcpyAsync(b->d_rows, rows.data(), rows.size() * sizeof(RowRef), cudaMemcpyHostToDevice, st));
     if (!wrows.empty())
         CB(cudaMemcpyAsync(b->d_wrows, wrows.data(), wrows.size() * sizeof(RowRef), cudaMemcpyHostToDevice, st));
@@ -1481,9 +1504,10 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (!b) return LBMGPU_ERR_INVALID;
     if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED3 && tile != LBMGPU_TILE_STAGED4 &&
-         tile != LBMGPU_TILE_ROWCTA) ||
+         tile != LBMGPU_TILE_ROWCTA && tile != LBMGPU_TILE_CHUNK) ||
         ctas_per_sm < 1 || ctas_per_sm > 16)
-        return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA or "
+        return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA, "
+                                            "LBMGPU_TILE_CHUNK or "
                                             "LBMGPU_TILE_STAGED3/4, and ctas_per_sm 1..16");
     BTRY(b, cudaSetDevice(b->p0.device));
     BTRY(b, cudaStreamSynchronize(b->sa));
@@ -1513,14 +1537,15 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaEvent_t e0, e1;
     BTRY(b, cudaEventCreate(&e0));
     BTRY(b, cudaEventCreate(&e1));
-    const int tiles[6] = {LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4};
+    const int tiles[7] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED3,
+                          LBMGPU_TILE_STAGED4};
     const int bpss[7] = {1, 2, 3, 4, 5, 6, 8};
     double best = 1e30;
     int btx = b->tile, bbps = b->bps;
     const BatchStep bst{(int)((b->t + 1) % ZONE_SLOTS), 0, 0};
     for (int tx : tiles)
         for (int bps : bpss) {
-            if (tx == LBMGPU_TILE_ROWCTA && bps != 1) continue;   // its grid is the row count
+            if ((tx == LBMGPU_TILE_ROWCTA || tx == LBMGPU_TILE_CHUNK) && bps != 1) continue;   // grid = rows / chunks
             const int grid = b->sms * bps;
             if (tx < 0) {
                 const int rc = set_bounds(b, grid);
