@@ -123,3 +123,29 @@ class Ensemble:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def main(argv=None) -> None:
+    """Run the first --members members of ensemble_members(256) for --steps
+    steps with a given bulk tiling (used for profiling):
+        python -m lbm_solver_3d_b200.ensemble --members 64 --steps 61 --tile 2"""
+    import argparse
+    from .workloads import ensemble_members
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=61)
+    ap.add_argument("--tile", type=int, default=2)
+    ap.add_argument("--ctas-per-sm", type=int, default=1)
+    ap.add_argument("--precision", default="fp32")
+    args = ap.parse_args(argv)
+    ps = ensemble_members(256)[: args.members]
+    for p in ps:
+        p.update(precision=args.precision)
+    with Ensemble(ps) as ens:
+        ens.set_tiling(args.tile, args.ctas_per_sm)
+        ens.run(args.steps)
+        print(f"{len(ps)} members, {ens.cells} nodes, {args.steps} steps, tile {args.tile}: ok")
+
+
+if __name__ == "__main__":
+    main()
