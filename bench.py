@@ -139,9 +139,18 @@ def cpu_baseline(p, seconds_target=15.0):
             break
         steps *= 2
     mlups = p.ncells * steps / t / 1e6
+    # the same sample on one thread (a bounded number of steps)
+    oracle.set_threads(1)
+    steps1 = max(1, min(steps, int(0.2 * seconds_target / max(t / steps * threads, 1e-9))))
+    t0 = time.perf_counter()
+    s.run(steps1)
+    t1 = time.perf_counter() - t0
+    oracle.set_threads(threads)
     return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
             "sample": f"{p.NX}x{p.NY}x{p.NZ} lattice, {steps} time steps after 1 warm-up step, "
-                      f"{threads} OpenMP threads, FP64 (the reference's only form)"}
+                      f"{threads} OpenMP threads, FP64 (the reference's only form)",
+            "one_thread": {"value": p.ncells * steps1 / t1 / 1e6, "unit": "MLUPS", "cores": 1,
+                           "sample": f"{steps1} further time steps on 1 thread"}}
 
 
 def run_reference_arm(args, p):
@@ -180,12 +189,20 @@ def run_reference_arm(args, p):
 
 
 def workload_config(args, p, reference=False):
-    return {"workload": f"{args.workload}: periodic {p.NX}x{p.NY}x{p.NZ} box, one squirmer "
-                        f"a={p.R:g} beta={p.beta:g} B1={p.B1:g} tau={p.tau:g}, seeded 3-D orientation"
-            if p.squirmer else f"{args.workload}: {p.NX}x{p.NY}x{p.NZ}",
+    if not p.squirmer:
+        what = f"{args.workload}: {p.NX}x{p.NY}x{p.NZ} duct, walls in y and z, body force fx={p.Fx:g}"
+    elif args.workload == "slit":
+        what = (f"slit: {p.NX}x{p.NY}x{p.NZ}, walls in y, one squirmer a={p.R:g} beta={p.beta:g} "
+                f"B1={p.B1:g} tau={p.tau:g} angle={p.angle:g}")
+    else:
+        what = (f"{args.workload}: periodic {p.NX}x{p.NY}x{p.NZ} box, one squirmer a={p.R:g} beta={p.beta:g} "
+                f"B1={p.B1:g} tau={p.tau:g}, seeded 3-D orientation")
+    return {"workload": what,
             "cells": p.ncells, "precision": "fp64" if reference else args.precision,
             "mass_correction_every": p.massCorrectionEvery,
-            "l2": "populations larger than L2 (126 MB); no flush",
+            "l2": ("populations larger than L2 (126 MB); no flush"
+                   if 38 * BYTES["fp64" if reference else args.precision] * p.ncells / 2 > 126e6
+                   else "populations fit in L2 (126 MB): L2-resident, the roofline fraction is not an HBM claim"),
             "parallelism": f"replica per GPU x{dist_env()[0]}"}
 
 
