@@ -216,8 +216,17 @@ int lbmgpu_mlp_train_epoch(lbmgpu_mlp* m, const int* order, int n_order, int bat
 /* Loss and gradient (LBMGPU_MLP_NPARAMS floats, may be NULL) over the whole
  * training set at the current parameters; no update. */
 int lbmgpu_mlp_loss_grad(lbmgpu_mlp* m, float* loss, float* grad);
-/* Inference: y[n][3] = net(x[n][4]). */
+/* Inference: y[n][3] = net(x[n][4]). BF16 networks run on the tensor cores
+ * through tensor memory (tcgen05.mma, 128 samples per CTA, FP32
+ * accumulators in TMEM); FP32 networks on the warp-tiled FP32 kernel.
+ * lbmgpu_mlp_forward_ex chooses the path: LBMGPU_MLP_PATH_AUTO (as above),
+ * LBMGPU_MLP_PATH_WARP (the warp-tiled training kernel's forward: mma.sync
+ * for BF16, FMA for FP32) or LBMGPU_MLP_PATH_TCGEN05 (BF16 networks only). */
+#define LBMGPU_MLP_PATH_AUTO 0
+#define LBMGPU_MLP_PATH_WARP 1
+#define LBMGPU_MLP_PATH_TCGEN05 2
 int lbmgpu_mlp_forward(lbmgpu_mlp* m, const float* x, int n, float* y);
+int lbmgpu_mlp_forward_ex(lbmgpu_mlp* m, const float* x, int n, float* y, int path);
 const char* lbmgpu_mlp_last_error(const lbmgpu_mlp* m);
 
 /* ---------------------------------------------------------------------------

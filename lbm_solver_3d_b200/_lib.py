@@ -89,6 +89,7 @@ SIGNATURES = {
                                     ctypes.POINTER(ctypes.c_float)]),
     "lbmgpu_mlp_loss_grad": (_I, [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "lbmgpu_mlp_forward": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float)]),
+    "lbmgpu_mlp_forward_ex": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float), _I]),
     "lbmgpu_mlp_last_error": (ctypes.c_char_p, [_P]),
     "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
     "lbmgpu_batch_destroy": (_I, [_P]),

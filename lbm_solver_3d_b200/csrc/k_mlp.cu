@@ -274,6 +274,188 @@ __global__ void k_mlp_adam(float* __restrict__ params, float* __restrict__ m1, f
     params[p] -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
 }
 
+// ---------------------------------------------------------------------------
+//  k_mlp_fwd_tc: BF16 inference on the fifth-generation tensor cores.
+//
+//  One CTA of 128 threads owns 128 samples: thread i is sample i, and row i
+//  of every product. Each layer is D[128 x N] = A[128 x K] . W^T with A (the
+//  activations) and W (the weights, [out][in]) in shared memory as BF16 and D
+//  in tensor memory (FP32, 64 columns allocated per CTA):
+//    thread 0 issues tcgen05.mma (kind::f16, cta_group::1, M = 128,
+//    N = 64 or 16, K = 16 per instruction) and tcgen05.commit to an mbarrier;
+//    every warp then reads its 32 rows of D with tcgen05.ld (32x32b), adds the
+//    bias, applies SiLU and writes the next layer's A in BF16.
+//  Operand layout in shared memory: K-major with no swizzle. The 8 x 8 BF16
+//  core matrices are 128 contiguous bytes (8 rows of 16 bytes). Row r, column k
+//  of an R-row operand is at byte ((k / 8) * R + r) * 16 + (k % 8) * 2, so the
+//  stride between 8-row groups (SBO) is 128 bytes and the stride between the
+//  two 8-column halves of a K = 16 step (LBO) is R * 16 bytes.
+//  Waits on the mbarrier are bounded; a timeout sets *err, and the tensor
+//  memory is released on every path.
+// ---------------------------------------------------------------------------
+constexpr int TC_M = 128;              // samples per CTA
+constexpr int TC_COLS = 64;            // tensor-memory columns (FP32 accumulators)
+
+struct TcSmem {
+    alignas(128) __nv_bfloat16 A[NH / 8][TC_M][8];       // activations, K-major core matrices
+    alignas(128) __nv_bfloat16 W1[PI_ / 8][NH][8];
+    alignas(128) __nv_bfloat16 W2[NH / 8][NH][8];
+    alignas(128) __nv_bfloat16 W3[NH / 8][NH][8];
+    alignas(128) __nv_bfloat16 W4[NH / 8][PO][8];
+    float b1[NH], b2[NH], b3[NH], b4[PO];
+    alignas(8) uint64_t mbar;
+    uint32_t tmem_base;
+};
+
+__device__ __forceinline__ uint64_t umma_desc(const void* smem, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+    uint64_t d = 0;
+    d |= (uint64_t)((a >> 4) & 0x3FFFu);                     // start address
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;       // leading dimension byte offset
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;       // stride dimension byte offset
+    d |= (uint64_t)1 << 46;                                  // descriptor version (sm_100)
+    return d;                                                // base offset 0, no swizzle
+}
+
+// BF16 x BF16 -> FP32, both operands K-major, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool tc_wait(uint64_t* m, uint32_t parity) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(m);
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// D[tmem] = A . W^T over K (multiple of 16), issued by one thread, completion on mbar
+__device__ __forceinline__ void tc_layer(uint32_t tmem, const void* A, const void* W, int K, int N, uint64_t* mbar) {
+    const uint32_t idesc = umma_idesc(N);
+    for (int k16 = 0; k16 < K / 16; ++k16) {
+        const uint64_t da = umma_desc((const char*)A + (size_t)k16 * 2 * TC_M * 16, TC_M * 16, 128);
+        const uint64_t db = umma_desc((const char*)W + (size_t)k16 * 2 * N * 16, N * 16, 128);
+        const uint32_t acc = k16 > 0;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}"
+            :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+            : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(mbar)) : "memory");
+}
+
+// 16 FP32 columns of this thread's row of D
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// W[out][in] (FP32, global) -> BF16 K-major core matrices with R rows (outputs)
+// and KP columns (inputs, zero-padded), rows >= rows_valid zero
+__device__ __forceinline__ void tc_load_w(__nv_bfloat16* dst, const float* w, int R, int rows_valid, int KP, int kin) {
+    for (int e = threadIdx.x; e < R * KP; e += blockDim.x) {
+        const int r = e / KP, k = e % KP;
+        const float v = (r < rows_valid && k < kin) ? w[r * kin + k] : 0.f;
+        dst[((size_t)(k / 8) * R + r) * 8 + (k % 8)] = __float2bfloat16_rn(v);
+    }
+}
+
+__global__ void __launch_bounds__(TC_M) k_mlp_fwd_tc(const float* __restrict__ params, const float* __restrict__ X,
+                                                     int n, float* __restrict__ Yout, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = blockIdx.x * TC_M + tid;
+
+    if (warp == 0) {   // tensor memory: one warp allocates, the same warp frees
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem_base)), "r"(TC_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"((uint32_t)__cvta_generic_to_shared(&S.mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_load_w(&S.W1[0][0][0], params + OFF_W1, NH, NH, PI_, NI);
+    tc_load_w(&S.W2[0][0][0], params + OFF_W2, NH, NH, NH, NH);
+    tc_load_w(&S.W3[0][0][0], params + OFF_W3, NH, NH, NH, NH);
+    tc_load_w(&S.W4[0][0][0], params + OFF_W4, PO, NO, NH, NH);
+    for (int e = tid; e < NH; e += TC_M) { S.b1[e] = params[OFF_B1 + e]; S.b2[e] = params[OFF_B2 + e]; S.b3[e] = params[OFF_B3 + e]; }
+    if (tid < PO) S.b4[tid] = tid < NO ? params[OFF_B4 + tid] : 0.f;
+    {   // this thread's input row, padded to 16
+        float xv[PI_];
+#pragma unroll
+        for (int k = 0; k < PI_; ++k) xv[k] = (k < NI && row < n) ? X[(size_t)row * NI + k] : 0.f;
+#pragma unroll
+        for (int c = 0; c < PI_ / 8; ++c)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) S.A[c][tid][j] = __float2bfloat16_rn(xv[c * 8 + j]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // operands visible to the tensor cores
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = S.tmem_base;
+    const uint32_t my_lanes = tmem + ((uint32_t)(warp * 32) << 16);
+
+    bool ok = true;
+    uint32_t phase = 0;
+    const void* Ws[3] = {&S.W1[0][0][0], &S.W2[0][0][0], &S.W3[0][0][0]};
+    const float* bs[3] = {S.b1, S.b2, S.b3};
+    for (int l = 0; l < 3 && ok; ++l) {
+        if (tid == 0) tc_layer(tmem, &S.A[0][0][0], Ws[l], l == 0 ? PI_ : NH, NH, &S.mbar);
+        ok = __all_sync(0xffffffffu, tc_wait(&S.mbar, phase));   // warp-uniform: tcgen05.ld is .sync.aligned
+        phase ^= 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (ok) {
+            float h[NH];
+#pragma unroll
+            for (int q = 0; q < NH / 16; ++q) tc_ld16(my_lanes + q * 16, h + q * 16);
+#pragma unroll
+            for (int j = 0; j < NH; ++j) h[j] = silu(h[j] + bs[l][j]);
+#pragma unroll
+            for (int c = 0; c < NH / 8; ++c)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) S.A[c][tid][j] = __float2bfloat16_rn(h[c * 8 + j]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ok = __syncthreads_and(ok);
+    }
+    if (ok) {
+        if (tid == 0) tc_layer(tmem, &S.A[0][0][0], &S.W4[0][0][0], NH, PO, &S.mbar);
+        ok = __all_sync(0xffffffffu, tc_wait(&S.mbar, phase));
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (ok) {
+            float y[16];
+            tc_ld16(my_lanes, y);
+            if (row < n)
+#pragma unroll
+                for (int o = 0; o < NO; ++o) Yout[(size_t)row * NO + o] = y[o] + S.b4[o];
+        }
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_COLS));
+}
+
 template <bool BF16, bool TRAIN>
 cudaError_t prepare_tile() {
     return cudaFuncSetAttribute(k_mlp_tile<BF16, TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
@@ -297,6 +479,7 @@ struct lbmgpu_mlp {
     float *xin = nullptr, *yout = nullptr;
     int xin_cap = 0, yout_cap = 0;      // floats
     float* small = nullptr;             // [0] loss, [1..NP] gradient
+    int* d_err = nullptr;               // tensor-core forward: a bounded wait gave up
     long long t = 0;                    // Adam steps taken
     float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
     std::string err;
@@ -392,6 +575,8 @@ int lbmgpu_mlp_create(int device, int bf16, lbmgpu_mlp** out) {
     if ((e = cudaMalloc(&m->m1, NP * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc");
     if ((e = cudaMalloc(&m->m2, NP * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc");
     if ((e = cudaMalloc(&m->small, (NP + 1) * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&m->d_err, sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc");
+    if ((e = cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemsetAsync(m->params, 0, NP * sizeof(float), m->stream)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemsetAsync(m->m1, 0, NP * sizeof(float), m->stream)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemsetAsync(m->m2, 0, NP * sizeof(float), m->stream)) != cudaSuccess) return bail(e, "memset");
@@ -404,7 +589,8 @@ int lbmgpu_mlp_destroy(lbmgpu_mlp* m) {
     if (!m) return LBMGPU_OK;
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
-    void* ptrs[] = {m->params, m->m1, m->m2, m->X, m->Y, m->idx, m->grad_part, m->loss_part, m->xin, m->yout, m->small};
+    void* ptrs[] = {m->params, m->m1, m->m2, m->X, m->Y, m->idx, m->grad_part, m->loss_part, m->xin, m->yout, m->small,
+                    m->d_err};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
@@ -507,24 +693,40 @@ int lbmgpu_mlp_loss_grad(lbmgpu_mlp* m, float* loss, float* grad) {
     return LBMGPU_OK;
 }
 
-int lbmgpu_mlp_forward(lbmgpu_mlp* m, const float* x, int n, float* y) {
+int lbmgpu_mlp_forward_ex(lbmgpu_mlp* m, const float* x, int n, float* y, int path) {
     if (!m || !x || !y || n < 1) return mfail(m, LBMGPU_ERR_INVALID, "need n >= 1 inputs");
+    if (path != LBMGPU_MLP_PATH_AUTO && path != LBMGPU_MLP_PATH_WARP && path != LBMGPU_MLP_PATH_TCGEN05)
+        return mfail(m, LBMGPU_ERR_INVALID, "unknown forward path");
+    if (path == LBMGPU_MLP_PATH_TCGEN05 && !m->bf16)
+        return mfail(m, LBMGPU_ERR_INVALID, "the tensor-memory path computes in BF16: create the network with bf16 = 1");
     MTRY(m, cudaSetDevice(m->device));
     MTRY(m, grow(&m->xin, &m->xin_cap, (long long)n * NI));
     MTRY(m, grow(&m->yout, &m->yout_cap, (long long)n * NO));
     MTRY(m, cudaMemcpyAsync(m->xin, x, (size_t)n * NI * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-    const int tiles = (n + MLP_T - 1) / MLP_T;
-    const size_t sm = sizeof(Smem);
-    if (m->bf16)
-        k_mlp_tile<true, false><<<tiles, MLP_THREADS, sm, m->stream>>>(m->params, m->xin, nullptr, nullptr, 0, n, 0.f,
-                                                                       nullptr, nullptr, m->yout);
-    else
-        k_mlp_tile<false, false><<<tiles, MLP_THREADS, sm, m->stream>>>(m->params, m->xin, nullptr, nullptr, 0, n, 0.f,
-                                                                        nullptr, nullptr, m->yout);
+    const bool tc = m->bf16 && path != LBMGPU_MLP_PATH_WARP;
+    if (tc) {
+        k_mlp_fwd_tc<<<(n + TC_M - 1) / TC_M, TC_M, sizeof(TcSmem), m->stream>>>(m->params, m->xin, n, m->yout, m->d_err);
+    } else {
+        const int tiles = (n + MLP_T - 1) / MLP_T;
+        const size_t sm = sizeof(Smem);
+        if (m->bf16)
+            k_mlp_tile<true, false><<<tiles, MLP_THREADS, sm, m->stream>>>(m->params, m->xin, nullptr, nullptr, 0, n,
+                                                                           0.f, nullptr, nullptr, m->yout);
+        else
+            k_mlp_tile<false, false><<<tiles, MLP_THREADS, sm, m->stream>>>(m->params, m->xin, nullptr, nullptr, 0, n,
+                                                                            0.f, nullptr, nullptr, m->yout);
+    }
     MTRY(m, cudaGetLastError());
+    int err = 0;
     MTRY(m, cudaMemcpyAsync(y, m->yout, (size_t)n * NO * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    if (tc) MTRY(m, cudaMemcpyAsync(&err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
     MTRY(m, cudaStreamSynchronize(m->stream));
+    if (err) return mfail(m, LBMGPU_ERR_WATCHDOG, "a tensor-core layer did not complete in time");
     return LBMGPU_OK;
+}
+
+int lbmgpu_mlp_forward(lbmgpu_mlp* m, const float* x, int n, float* y) {
+    return lbmgpu_mlp_forward_ex(m, x, n, y, LBMGPU_MLP_PATH_AUTO);
 }
 
 const char* lbmgpu_mlp_last_error(const lbmgpu_mlp* m) { return m ? m->err.c_str() : g_mlp_error.c_str(); }

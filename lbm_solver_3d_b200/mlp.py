@@ -74,10 +74,14 @@ class MLP:
         self._check(self.lib.lbmgpu_mlp_loss_grad(self.h, ctypes.byref(loss), _fp(g)), self.h)
         return loss.value, g
 
-    def forward(self, x) -> np.ndarray:
+    PATH_AUTO, PATH_WARP, PATH_TCGEN05 = 0, 1, 2
+
+    def forward(self, x, path: int = 0) -> np.ndarray:
+        """Inference. path: PATH_AUTO (tensor memory for BF16 networks, FP32
+        FMA otherwise), PATH_WARP (the warp-tiled kernel), PATH_TCGEN05."""
         x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 4)
         y = np.empty((x.shape[0], 3), np.float32)
-        self._check(self.lib.lbmgpu_mlp_forward(self.h, _fp(x), x.shape[0], _fp(y)), self.h)
+        self._check(self.lib.lbmgpu_mlp_forward_ex(self.h, _fp(x), x.shape[0], _fp(y), int(path)), self.h)
         return y
 
     def close(self) -> None:

@@ -123,3 +123,30 @@ def test_training_is_deterministic():
         outs.append(net.params())
         net.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [5, 128, 1001])
+def test_tensor_memory_forward(n):
+    """BF16 inference through tcgen05.mma / tensor memory (128 samples per CTA)
+    against the warp-tiled mma.sync path (same BF16 rounding points, FP32
+    accumulation in another order: within 1e-3) and the float64 oracle
+    (within the BF16 tolerance, 2e-2)."""
+    from lbm_solver_3d_b200.mlp import MLP
+    from lbm_solver_3d_b200._lib import LbmgpuError
+    x, _ = problem(n, 30 + n)
+    th = O.init_params(11).astype(np.float32)
+    net = MLP(bf16=True, params=th)
+    tc = net.forward(x, path=MLP.PATH_TCGEN05)
+    warp = net.forward(x, path=MLP.PATH_WARP)
+    auto = net.forward(x)
+    ref = O.forward(th.astype(np.float64), x)
+    print(f"n={n}: tcgen05 vs warp {rel_l2(tc, warp):.2e}, vs oracle {rel_l2(tc, ref):.2e}")
+    assert np.array_equal(auto, tc)
+    assert rel_l2(tc, warp) < 1e-3
+    assert rel_l2(tc, ref) < 2e-2
+    net.close()
+    f32 = MLP(bf16=False, params=th)
+    with pytest.raises(LbmgpuError, match="BF16"):
+        f32.forward(x, path=MLP.PATH_TCGEN05)
+    f32.close()
