@@ -152,6 +152,18 @@ int lbmgpu_traj_rows(lbmgpu_handle* h, double* rows, int max_rows, int* nrows, l
 int lbmgpu_get_populations(lbmgpu_handle* h, double* f);
 int lbmgpu_set_populations(lbmgpu_handle* h, const double* f);
 
+/* Checkpoint / restart (no counterpart in the reference, which cannot resume
+ * a run). A checkpoint is the complete device state of a lattice in a host
+ * buffer: the stored populations (storage form and AA parity as they are),
+ * flags, rho/u of the last step, the squirmer state with its zones, pending
+ * mass correction and counters, the boundary-link list and the trajectory
+ * ring. Loading it into a lattice created with the same parameters continues
+ * the run bit for bit. _size gives the bytes _save needs; _load checks the
+ * lattice sizes, storage form and squirmer presence and rejects a mismatch. */
+int lbmgpu_checkpoint_size(lbmgpu_handle* h, size_t* bytes);
+int lbmgpu_checkpoint_save(lbmgpu_handle* h, void* buf, size_t len);
+int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len);
+
 /* Overwrite the rigid-body state X, e, U, W (seeded parity cases, restart).
  * The lattice mapping is not changed. */
 int lbmgpu_set_squirmer_state(lbmgpu_handle* h, const double X[3], const double e[3],

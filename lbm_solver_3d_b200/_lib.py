@@ -91,6 +91,9 @@ SIGNATURES = {
     "lbmgpu_mlp_forward": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float)]),
     "lbmgpu_mlp_forward_ex": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float), _I]),
     "lbmgpu_mlp_last_error": (ctypes.c_char_p, [_P]),
+    "lbmgpu_checkpoint_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
+    "lbmgpu_checkpoint_save": (_I, [_P, _P, ctypes.c_size_t]),
+    "lbmgpu_checkpoint_load": (_I, [_P, _P, ctypes.c_size_t]),
     "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
     "lbmgpu_batch_destroy": (_I, [_P]),
     "lbmgpu_batch_run": (_I, [_P, _I]),

@@ -918,6 +918,137 @@ int lbmgpu_traj_rows(lbmgpu_handle* h, double* rows, int max_rows, int* nrows, l
     return LBMGPU_OK;
 }
 
+// ---- checkpoint / restart --------------------------------------------------
+// A checkpoint is the complete device state of a lattice as stored: the
+// populations in their storage form and AA parity, flags, the moments of the
+// last step, the squirmer state (with its zones, pending mass correction and
+// trajectory counters), the boundary-link list and the trajectory ring. A
+// lattice created with the same parameters and loaded from it continues bit
+// for bit as the saved one would have.
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, precision;
+    int32_t nx, ny, nz, has_sq;
+    int64_t t_main, traj_read;
+    int32_t pending_corr, n_links;
+    uint64_t f_bytes, sq_bytes;
+};
+constexpr char CKPT_MAGIC[8] = {'L', 'B', 'M', 'G', 'P', 'U', 'C', 'K'};
+
+size_t ckpt_bytes(const lbmgpu_handle* h, int n_links) {
+    const size_t N = h->L.N;
+    size_t b = sizeof(CkptHeader) + (size_t)Q * N * h->esize + N + 4 * N * sizeof(double) + sizeof(SqState);
+    if (h->has_sq) b += (size_t)n_links * sizeof(int) + (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double);
+    return b;
+}
+int ckpt_links(lbmgpu_handle* h, int* n_links) {
+    SqState s;
+    CUDA_TRY(h, cudaMemcpyAsync(&s, h->sq, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    *n_links = h->has_sq ? std::max(0, s.n_links) : 0;
+    return LBMGPU_OK;
+}
+}  // namespace
+
+int lbmgpu_checkpoint_size(lbmgpu_handle* h, size_t* bytes) {
+    if (!h || !bytes) return LBMGPU_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->p.device));
+    int nl = 0;
+    const int rc = ckpt_links(h, &nl);
+    if (rc) return rc;
+    *bytes = ckpt_bytes(h, nl);
+    return LBMGPU_OK;
+}
+
+int lbmgpu_checkpoint_save(lbmgpu_handle* h, void* buf, size_t len) {
+    if (!h || !buf) return LBMGPU_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->p.device));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (h->zs) CUDA_TRY(h, cudaStreamSynchronize(h->zs));
+    int nl = 0;
+    int rc = ckpt_links(h, &nl);
+    if (rc) return rc;
+    if (len < ckpt_bytes(h, nl)) return fail(h, LBMGPU_ERR_INVALID, "checkpoint buffer too small (lbmgpu_checkpoint_size)");
+    const size_t N = h->L.N;
+    CkptHeader hd{};
+    std::memcpy(hd.magic, CKPT_MAGIC, 8);
+    hd.version = 1; hd.precision = (uint32_t)h->p.precision;
+    hd.nx = h->p.nx; hd.ny = h->p.ny; hd.nz = h->p.nz; hd.has_sq = h->has_sq;
+    hd.t_main = h->t_main; hd.traj_read = h->traj_read; hd.pending_corr = h->pending_corr ? 1 : 0;
+    hd.n_links = nl;
+    hd.f_bytes = (uint64_t)Q * N * h->esize; hd.sq_bytes = sizeof(SqState);
+    char* p = static_cast<char*>(buf);
+    std::memcpy(p, &hd, sizeof(hd)); p += sizeof(hd);
+    cudaStream_t st = h->stream;
+    auto d2h = [&](const void* src, size_t n) {
+        const cudaError_t e = cudaMemcpyAsync(p, src, n, cudaMemcpyDeviceToHost, st);
+        p += n;
+        return e;
+    };
+    CUDA_TRY(h, d2h(h->f, hd.f_bytes));
+    CUDA_TRY(h, d2h(h->flag, N));
+    CUDA_TRY(h, d2h(h->rho, N * sizeof(double)));
+    CUDA_TRY(h, d2h(h->ux, N * sizeof(double)));
+    CUDA_TRY(h, d2h(h->uy, N * sizeof(double)));
+    CUDA_TRY(h, d2h(h->uz, N * sizeof(double)));
+    CUDA_TRY(h, d2h(h->sq, sizeof(SqState)));
+    if (h->has_sq) {
+        if (nl) CUDA_TRY(h, d2h(h->links, (size_t)nl * sizeof(int)));
+        CUDA_TRY(h, d2h(h->traj, (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double)));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return LBMGPU_OK;
+}
+
+int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len) {
+    if (!h || !buf) return LBMGPU_ERR_INVALID;
+    if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
+    if (len < sizeof(CkptHeader)) return fail(h, LBMGPU_ERR_INVALID, "not a checkpoint (too short)");
+    CkptHeader hd;
+    std::memcpy(&hd, buf, sizeof(hd));
+    if (std::memcmp(hd.magic, CKPT_MAGIC, 8) != 0 || hd.version != 1)
+        return fail(h, LBMGPU_ERR_INVALID, "not a checkpoint of this library (magic/version)");
+    if (hd.nx != h->p.nx || hd.ny != h->p.ny || hd.nz != h->p.nz || (int)hd.precision != h->p.precision ||
+        hd.has_sq != h->has_sq || hd.sq_bytes != sizeof(SqState) ||
+        hd.f_bytes != (uint64_t)Q * h->L.N * h->esize)
+        return fail(h, LBMGPU_ERR_INVALID, "checkpoint of another lattice (sizes, precision or squirmer differ)");
+    if (hd.n_links < 0 || hd.n_links > h->link_cap) return fail(h, LBMGPU_ERR_INVALID, "checkpoint link list too long");
+    if (len < ckpt_bytes(h, hd.n_links)) return fail(h, LBMGPU_ERR_INVALID, "checkpoint truncated");
+    CUDA_TRY(h, cudaSetDevice(h->p.device));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (h->zs) CUDA_TRY(h, cudaStreamSynchronize(h->zs));
+    const size_t N = h->L.N;
+    const char* p = static_cast<const char*>(buf) + sizeof(hd);
+    cudaStream_t st = h->stream;
+    auto h2d = [&](void* dst, size_t n) {
+        const cudaError_t e = cudaMemcpyAsync(dst, p, n, cudaMemcpyHostToDevice, st);
+        p += n;
+        return e;
+    };
+    CUDA_TRY(h, h2d(h->f, hd.f_bytes));
+    CUDA_TRY(h, h2d(h->flag, N));
+    CUDA_TRY(h, h2d(h->rho, N * sizeof(double)));
+    CUDA_TRY(h, h2d(h->ux, N * sizeof(double)));
+    CUDA_TRY(h, h2d(h->uy, N * sizeof(double)));
+    CUDA_TRY(h, h2d(h->uz, N * sizeof(double)));
+    CUDA_TRY(h, h2d(h->sq, sizeof(SqState)));
+    if (h->has_sq) {
+        if (hd.n_links) {
+            CUDA_TRY(h, h2d(h->links, (size_t)hd.n_links * sizeof(int)));
+            k_scatter_slots<<<64, 256, 0, st>>>(h->links, hd.n_links, h->linkslot);
+            ++h->launches;
+        }
+        CUDA_TRY(h, h2d(h->traj, (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double)));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    CUDA_TRY(h, cudaGetLastError());
+    h->t_main = hd.t_main;
+    h->traj_read = hd.traj_read;
+    h->pending_corr = hd.pending_corr != 0;
+    return LBMGPU_OK;
+}
+
 int lbmgpu_get_populations(lbmgpu_handle* h, double* f) {
     if (!h || !f) return LBMGPU_ERR_INVALID;
     CUDA_TRY(h, cudaSetDevice(h->p.device));

@@ -14,9 +14,12 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <fstream>
+#include <iterator>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "output.hpp"
 #include "params.hpp"
@@ -75,23 +78,48 @@ int runSimulation(const Params& p) {
     const lbmgpu_params cp = p.toC();
     if (lbmgpu_create(&cp, &dev.h) != LBMGPU_OK)
         throw std::runtime_error(std::string("device: ") + lbmgpu_last_error(nullptr));
+    int t = 0;
+    if (!p.restart.empty()) {   // continue a checkpointed run: same parameters, state from the file
+        std::ifstream in(p.restart, std::ios::binary);
+        if (!in) throw std::runtime_error("cannot read '" + p.restart + "'");
+        const std::vector<char> buf((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+        dev.check(lbmgpu_checkpoint_load(dev.h, buf.data(), buf.size()));
+        long long t0 = 0;
+        dev.check(lbmgpu_time(dev.h, &t0));
+        t = (int)t0;
+        std::printf("restarted from %s at t=%d\n", p.restart.c_str(), t);
+    }
     std::unique_ptr<TrajectoryFile> traj;
-    if (p.squirmer) traj = std::make_unique<TrajectoryFile>(base + "_traj.dat");
+    if (p.squirmer) traj = std::make_unique<TrajectoryFile>(base + "_traj.dat", !p.restart.empty());
     const double nu = (p.tau - 0.5) / 3.0;
 
     const auto t0 = std::chrono::steady_clock::now();
     double prevSum = 0.0;
-    int t = 0;
     bool converged = false;
     while (t < p.steps) {
         // the next step at which the host has something to do (main.cpp:60-87)
         long long next = std::min<long long>(p.steps, (long long)(t / p.printEvery + 1) * p.printEvery);
         if (p.vtkEvery > 0) next = std::min<long long>(next, (long long)(t / p.vtkEvery + 1) * p.vtkEvery);
         if (p.squirmer) next = std::min<long long>(next, t + kTrajRing * p.trajEvery);
+        if (p.checkpointEvery > 0)
+            next = std::min<long long>(next, (long long)(t / p.checkpointEvery + 1) * p.checkpointEvery);
         dev.check(lbmgpu_run(dev.h, (int)(next - t)));
         t = (int)next;
         if (p.squirmer) drainTrajectory(dev, *traj);
         if (p.vtkEvery > 0 && t % p.vtkEvery == 0) writeVtk(dev.fields(p), base + "_" + std::to_string(t) + ".vtk");
+        if (p.checkpointEvery > 0 && t % p.checkpointEvery == 0) {
+            if (traj) traj->flush();
+            size_t n = 0;
+            dev.check(lbmgpu_checkpoint_size(dev.h, &n));
+            std::vector<char> buf(n);
+            dev.check(lbmgpu_checkpoint_save(dev.h, buf.data(), n));
+            const std::string path = base + "_checkpoint.bin", tmp = path + ".tmp";
+            std::ofstream out(tmp, std::ios::binary);
+            out.write(buf.data(), (std::streamsize)n);
+            out.close();
+            if (!out || std::rename(tmp.c_str(), path.c_str()) != 0)
+                throw std::runtime_error("cannot write '" + path + "'");
+        }
         if (t % p.printEvery == 0) {
             if (p.squirmer) {
                 const lbmgpu_squirmer s = dev.squirmer();

@@ -60,10 +60,10 @@ void writeVtk(const Fields& F, const std::string& path) {
 }
 
 // io.cpp:72-83
-TrajectoryFile::TrajectoryFile(const std::string& path) {
-    fp_ = std::fopen(path.c_str(), "w");
+TrajectoryFile::TrajectoryFile(const std::string& path, bool append) {
+    fp_ = std::fopen(path.c_str(), append ? "a" : "w");
     if (!fp_) throw std::runtime_error("cannot write '" + path + "'");
-    std::fprintf(fp_, "# t X Y Z ex ey ez Ux Uy Uz Wx Wy Wz Fwall_y Fwall_z\n");
+    if (!append) std::fprintf(fp_, "# t X Y Z ex ey ez Ux Uy Uz Wx Wy Wz Fwall_y Fwall_z\n");
 }
 TrajectoryFile::~TrajectoryFile() {
     if (fp_) std::fclose(fp_);

@@ -31,7 +31,7 @@ void writeVtk(const Fields& F, const std::string& path);     // throws std::runt
 
 class TrajectoryFile {
 public:
-    explicit TrajectoryFile(const std::string& path);
+    explicit TrajectoryFile(const std::string& path, bool append = false);
     ~TrajectoryFile();
     void append(const double* row);   // 15 values (see lbmgpu_traj_rows)
     void flush();

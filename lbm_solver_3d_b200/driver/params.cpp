@@ -70,6 +70,8 @@ const std::map<std::string, Setter>& keyTable() {
         {"eps", asReal(&Params::eps)}, {"hc", asReal(&Params::hc)}, {"hmin", asReal(&Params::hmin)},
         {"ex", asAxis(&Params::ex)}, {"ey", asAxis(&Params::ey)}, {"ez", asAxis(&Params::ez)},
         {"device", asInt(&Params::device)},
+        {"checkpoint_every", asInt(&Params::checkpointEvery)},
+        {"restart", asText(&Params::restart)},
         {"precision",
          [](Params& p, const std::string& v) {
              const std::string l = lowercase(strip(v));

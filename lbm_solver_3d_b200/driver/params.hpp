@@ -5,7 +5,8 @@
 //  validation rules and messages as lbm::Params (src/utils/params.hpp:14-63,
 //  src/utils/params.cpp:37-157), so existing input decks and command lines run
 //  unchanged. Added keys: precision (fp64 | fp32 | fp16), ex/ey/ez (a 3-D
-//  initial orientation instead of `angle`) and device.
+//  initial orientation instead of `angle`), device, checkpoint_every and
+//  restart (checkpoint / restart of the whole device state).
 // ============================================================================
 #pragma once
 #include <cstdio>
@@ -33,6 +34,8 @@ struct Params {
     bool useOrientation = false;
     double ex = 0.0, ey = 0.0, ez = 0.0;
     int device = 0;
+    int checkpointEvery = 0;          // write <prefix>_checkpoint.bin every this many steps (0: never)
+    std::string restart;              // continue from this checkpoint file
 
     void set(const std::string& key, const std::string& value);  // throws std::runtime_error
     void loadFile(const std::string& path);

@@ -21,7 +21,7 @@ PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
 
 # Keys beyond the reference's set: storage precision and a 3-D initial
 # orientation (the reference only takes an in-plane angle, squirmer.cpp:26-27).
-EXTRA_KEYS = ("precision", "ex", "ey", "ez", "device")
+EXTRA_KEYS = ("precision", "ex", "ey", "ez", "device", "checkpoint_every", "restart")
 
 
 class ParamError(RuntimeError):
@@ -103,6 +103,8 @@ class Params:
     precision: str = "fp64"
     orientation: tuple | None = None
     device: int = 0
+    checkpoint_every: int = 0   # the driver writes <prefix>_checkpoint.bin every this many steps
+    restart: str = ""           # the driver continues from this checkpoint file
 
     # ---- key = value (params.cpp:37-75) ----
     def set(self, key: str, v: str) -> None:
@@ -150,6 +152,8 @@ class Params:
                 o["xyz".index(k[1])] = _stod(v)
                 self.orientation = tuple(o)
             elif k == "device": self.device = _stoi(v)
+            elif k == "checkpoint_every": self.checkpoint_every = _stoi(v)
+            elif k == "restart": self.restart = v.strip()
             else:
                 raise ParamError(f"unknown parameter '{k}'")
         except ValueError:
@@ -273,6 +277,10 @@ class Params:
             if self.orientation is not None:
                 kv += [f"ex={_fmt(self.orientation[0])}", f"ey={_fmt(self.orientation[1])}",
                        f"ez={_fmt(self.orientation[2])}"]
+            if self.checkpoint_every:
+                kv.append(f"checkpoint_every={self.checkpoint_every}")
+            if self.restart:
+                kv.append(f"restart={self.restart}")
         return kv
 
 

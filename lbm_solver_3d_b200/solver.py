@@ -131,6 +131,27 @@ class Solver:
         assert f.size == Q * self.N
         check(self.lib.lbmgpu_set_populations(self.h, dptr(f)), self.h)
 
+    # ---- checkpoint / restart ----
+    def checkpoint(self) -> bytes:
+        """The complete device state of the lattice (lbmgpu_checkpoint_save)."""
+        n = ctypes.c_size_t()
+        check(self.lib.lbmgpu_checkpoint_size(self.h, ctypes.byref(n)), self.h)
+        buf = ctypes.create_string_buffer(n.value)
+        check(self.lib.lbmgpu_checkpoint_save(self.h, buf, n.value), self.h)
+        return buf.raw
+
+    def restore(self, data: bytes) -> None:
+        """Continue from a checkpoint of a lattice with the same parameters."""
+        check(self.lib.lbmgpu_checkpoint_load(self.h, data, len(data)), self.h)
+
+    def save(self, path) -> None:
+        with open(path, "wb") as fh:
+            fh.write(self.checkpoint())
+
+    def load(self, path) -> None:
+        with open(path, "rb") as fh:
+            self.restore(fh.read())
+
     def close(self) -> None:
         if getattr(self, "h", None):
             if getattr(self, "_owned", True):

@@ -186,3 +186,23 @@ def test_driver_reproduces_shipped_channel_trajectory(tmp_path):
     assert np.all(np.abs(rows[:, 7:] - ref[:, 7:])[big] / np.abs(ref[:, 7:])[big] <= 5.1e-7)
     assert (tmp_path / "channel_neutral_final.vtk").exists()
     assert (tmp_path / "channel_neutral_squirmer.dat").exists()
+
+
+def test_driver_checkpoint_and_restart(tmp_path):
+    """The drop-in driver with checkpoint_every writes <prefix>_checkpoint.bin;
+    a second run with restart= continues from it and writes the same
+    trajectory rows and final squirmer state as one uninterrupted run."""
+    deck = dict(nx=40, ny=26, nz=22, tau=1.0, walls_y=1, walls_z=0, squirmer=1, radius=4.5, b1=0.015, beta=-2,
+                angle=20, planar=1, print_every=100, traj_every=20)
+    full = tmp_path / "full"; full.mkdir()
+    run_driver(full, deck, steps=400, prefix="run")
+    part = tmp_path / "part"; part.mkdir()
+    run_driver(part, deck, steps=200, prefix="run", checkpoint_every=200)
+    ck = part / "run_checkpoint.bin"
+    assert ck.exists()
+    out = run_driver(part, deck, steps=400, prefix="run", restart=str(ck))
+    assert "restarted from" in out and "t=200" in out
+    a = np.loadtxt(full / "run_traj.dat")
+    b = np.loadtxt(part / "run_traj.dat")
+    assert a.shape == b.shape and np.array_equal(a, b)
+    assert (full / "run_squirmer.dat").read_text() == (part / "run_squirmer.dat").read_text()

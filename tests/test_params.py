@@ -50,6 +50,8 @@ def test_extra_keys():
     assert p.precision == "fp32" and p.orientation == (0.0, 1.0, 0.0)
     with pytest.raises(ParamError, match="precision must be one of"):
         Params().set("precision", "fp8")
+    q = Params().update(checkpoint_every=500, restart="run_checkpoint.bin")
+    assert q.checkpoint_every == 500 and q.restart == "run_checkpoint.bin"
 
 
 def test_reference_parser_agrees(oracle_mod):
