@@ -317,6 +317,8 @@ int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
  *     ctas_per_sm unused);
  *   tile = LBMGPU_TILE_CHUNK: one warp per 32 consecutive nodes of a row
  *     (grid = chunks / 4, ctas_per_sm unused);
+ *   tile = LBMGPU_TILE_CHUNKP: the same chunks walked by persistent warps
+ *     (grid = ctas_per_sm x SMs, 4 warps per CTA);
  *   tile = LBMGPU_TILE_STAGED3 / _STAGED4: each CTA owns a contiguous range
  *     of rows (equal node counts); a producer warp stages every row's
  *     populations and flags in shared memory with bulk asynchronous copies,
@@ -324,6 +326,7 @@ int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
  * ctas_per_sm (1..16): the grid is that many CTAs per SM. */
 #define LBMGPU_TILE_ROWCTA 1
 #define LBMGPU_TILE_CHUNK 2
+#define LBMGPU_TILE_CHUNKP 3
 #define LBMGPU_TILE_STAGED3 (-3)
 #define LBMGPU_TILE_STAGED4 (-4)
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm);

@@ -227,6 +227,65 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_c
     }
 }
 
+// k_bulk_chunkp<S, PAR, MACRO>: the chunks of k_bulk_chunk walked by persistent
+// warps (grid = SMs x CTAs per SM, 4 warps per CTA): warp g takes chunks
+// g, g + G, g + 2G, ... (G = all warps). The member records are copied only
+// when the member changes, and the next chunk's descriptor is loaded while
+// the current chunk is updated, so a warp's start-up latency is paid once.
+template <class S, int PAR, bool MACRO>
+__global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_chunkp(
+    const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args, const ChunkRef* __restrict__ chunks,
+    int nchunks, double* __restrict__ chunk_part, BatchStep st) {
+    __shared__ __align__(16) Lattice sL[CHUNK_WARPS];
+    __shared__ __align__(16) StreamArgs sA[CHUNK_WARPS];
+    __shared__ ZoneBox sZ[CHUNK_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = gridDim.x * CHUNK_WARPS;
+    int c = blockIdx.x * CHUNK_WARPS + w;
+    int cur_m = -1;
+    ChunkRef next{};
+    if (c < nchunks) next = chunks[c];
+    for (; c < nchunks; c += G) {
+        const ChunkRef cr = next;
+        if (c + G < nchunks) next = chunks[c + G];   // in flight while this chunk is updated
+        if (cr.m != cur_m) {                          // warp-uniform
+            __syncwarp();
+            constexpr int NL = (int)(sizeof(Lattice) / 4), NA = (int)(sizeof(StreamArgs) / 4);
+            const uint32_t* srcl = reinterpret_cast<const uint32_t*>(lat + cr.m);
+            uint32_t* dstl = reinterpret_cast<uint32_t*>(&sL[w]);
+            for (int k = lane; k < NL; k += 32) dstl[k] = srcl[k];
+            const uint32_t* srca = reinterpret_cast<const uint32_t*>(args + cr.m);
+            uint32_t* dsta = reinterpret_cast<uint32_t*>(&sA[w]);
+            for (int k = lane; k < NA; k += 32) {
+                uint32_t v = srca[k];
+                if (k == (int)(offsetof(StreamArgs, zslot) / 4)) v = (uint32_t)st.zslot;
+                if (k == (int)(offsetof(StreamArgs, do_mass) / 4)) v = (uint32_t)st.do_mass;
+                if (k == (int)(offsetof(StreamArgs, apply_corr) / 4)) v = (uint32_t)st.apply_corr;
+                dsta[k] = v;
+            }
+            if (lane == 0) sZ[w] = args[cr.m].sq->zone[st.zslot];
+            __syncwarp();
+            cur_m = cr.m;
+        }
+        const Lattice& L = sL[w];
+        const StreamArgs& a = sA[w];
+        NodeSums sums;
+        const int x = cr.x0 + lane;
+        if (x < L.nx) {
+            const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)cr.y + (unsigned)L.ny * (unsigned)cr.z);
+            const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, cr.y, cr.z);
+            if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, cr.y, cr.z, 0, 0, MACRO, sums);
+        }
+        if (st.do_mass || MACRO) {
+            chunk_reduce(sums);
+            if (lane == 0) {
+                double* o = chunk_part + (size_t)c * BLOCK_PART;
+                o[0] = sums.fw[0]; o[1] = sums.fw[1]; o[2] = sums.fw[2]; o[3] = sums.mass;
+            }
+        }
+    }
+}
+
 // row partial = its chunk partials added in order, from 0 (one thread per row)
 static __global__ void k_fold_chunks(const RowChunks* __restrict__ rc, int nrows, const double* __restrict__ chunk_part,
                               double* __restrict__ row_part) {

@@ -68,7 +68,8 @@ struct Launchers {
     // the rows away from walls through shared-memory stages (k_bulk_staged)
     void (*batch_staged)(int par, bool macro, int nst, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
     // one warp per 32-node chunk (k_bulk_chunk, then k_fold_chunks when summing)
-    void (*batch_chunk)(int par, bool macro, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    void (*batch_chunk)(int par, bool macro, bool sums, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    int (*chunkp_ctas_per_sm)();   // resident CTAs per SM of the persistent chunk kernel
     // one CTA per row (k_bulk_rowcta): rows away from walls, or next to one
     void (*batch_rowcta)(int par, bool macro, bool wallrows, const BatchArgs& b, BatchStep st, cudaStream_t s);
     size_t esize;

@@ -132,13 +132,34 @@ static void chunk_one(bool sums, const BatchArgs& b, BatchStep st, cudaStream_t 
     if (sums) k_fold_chunks<<<(b.nrows + 255) / 256, 256, 0, s>>>(b.rowchunks, b.nrows, b.chunk_part, b.row_part);
 }
 
+template <class S, int PAR, bool MACRO>
+static void chunkp_one(int grid, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    if (b.nchunks == 0) return;
+    k_bulk_chunkp<S, PAR, MACRO><<<grid, 32 * CHUNK_WARPS, 0, s>>>(b.lat, b.args, b.chunks, b.nchunks, b.chunk_part, st);
+    if (sums) k_fold_chunks<<<(b.nrows + 255) / 256, 256, 0, s>>>(b.rowchunks, b.nrows, b.chunk_part, b.row_part);
+}
+
 template <class S>
-static void batch_chunk_launch(int par, bool macro, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s) {
-    switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
+static int chunkp_occupancy() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_chunkp<S, 1, false>, 32 * CHUNK_WARPS, 0) != cudaSuccess)
+        return 4;
+    return n > 0 ? n : 1;
+}
+
+// grid > 0: the persistent variant with that many CTAs
+template <class S>
+static void batch_chunk_launch(int par, bool macro, bool sums, int grid, const BatchArgs& b, BatchStep st,
+                               cudaStream_t s) {
+    switch ((grid > 0 ? 4 : 0) | (par ? 2 : 0) | (macro ? 1 : 0)) {
         case 0: chunk_one<S, 0, false>(sums, b, st, s); break;
         case 1: chunk_one<S, 0, true>(sums, b, st, s); break;
         case 2: chunk_one<S, 1, false>(sums, b, st, s); break;
-        default: chunk_one<S, 1, true>(sums, b, st, s); break;
+        case 3: chunk_one<S, 1, true>(sums, b, st, s); break;
+        case 4: chunkp_one<S, 0, false>(grid, sums, b, st, s); break;
+        case 5: chunkp_one<S, 0, true>(grid, sums, b, st, s); break;
+        case 6: chunkp_one<S, 1, false>(grid, sums, b, st, s); break;
+        default: chunkp_one<S, 1, true>(grid, sums, b, st, s); break;
     }
 }
 
@@ -220,6 +241,7 @@ static Launchers make_launchers() {
     l.batch_staged = &batch_staged_launch<S>;
     l.batch_rowcta = &batch_rowcta_launch<S>;
     l.batch_chunk = &batch_chunk_launch<S>;
+    l.chunkp_ctas_per_sm = &chunkp_occupancy<S>;
     l.esize = sizeof(typename S::T);
     return l;
 }

@@ -1230,7 +1230,7 @@ struct lbmgpu_batch {
     // tiling of the bulk launch (autotuned): tile > 0 is k_bulk_batch with that
     // many threads per row, tile < 0 is k_bulk_staged with -tile stages;
     // the grid is bps CTAs per SM
-    int tile = LBMGPU_TILE_CHUNK, bps = 4;
+    int tile = LBMGPU_TILE_CHUNKP, bps = 4;   // bps: resident CTAs per SM, set at creation
     int* d_bounds = nullptr;       // staged kernel: row range of each CTA
     ChunkRef* d_chunks = nullptr;  // chunk kernel
     RowChunks* d_rowchunks = nullptr;
@@ -1313,7 +1313,8 @@ int set_bounds(lbmgpu_batch* b, int grid) {
 void launch_bulk(lbmgpu_batch* b, int tile, int grid, int par, bool macro, BatchStep bst, cudaStream_t s) {
     if (tile < 0) b->lz->batch_staged(par, macro, -tile, grid, b->ba, bst, s);
     else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, false, b->ba, bst, s);
-    else if (tile == LBMGPU_TILE_CHUNK) b->lz->batch_chunk(par, macro, macro || bst.do_mass, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_CHUNK) b->lz->batch_chunk(par, macro, macro || bst.do_mass, 0, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_CHUNKP) b->lz->batch_chunk(par, macro, macro || bst.do_mass, grid, b->ba, bst, s);
     else b->lz->batch_bulk(par, macro, false, tile, grid, b->ba, bst, s);
 }
 
@@ -1563,6 +1564,7 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
     const int base = std::lcm(2, ZONE_SLOTS);
     b->corr_in_graph = b->has_sq && k > 0 && std::lcm(base, k) <= MAX_PERIOD;
     b->period = b->corr_in_graph ? std::lcm(base, k) : base;
+    b->bps = std::min(16, b->lz->chunkp_ctas_per_sm());   // one wave of the persistent chunk kernel
     if (set_bounds(b, b->sms * b->bps) != LBMGPU_OK) return bail(LBMGPU_ERR_CUDA);
 #undef CB
     *out = b;
@@ -1635,7 +1637,7 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (!b) return LBMGPU_ERR_INVALID;
     if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED3 && tile != LBMGPU_TILE_STAGED4 &&
-         tile != LBMGPU_TILE_ROWCTA && tile != LBMGPU_TILE_CHUNK) ||
+         tile != LBMGPU_TILE_ROWCTA && tile != LBMGPU_TILE_CHUNK && tile != LBMGPU_TILE_CHUNKP) ||
         ctas_per_sm < 1 || ctas_per_sm > 16)
         return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA, "
                                             "LBMGPU_TILE_CHUNK or "
@@ -1668,8 +1670,8 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaEvent_t e0, e1;
     BTRY(b, cudaEventCreate(&e0));
     BTRY(b, cudaEventCreate(&e1));
-    const int tiles[7] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_ROWCTA, 32, 64, 128, LBMGPU_TILE_STAGED3,
-                          LBMGPU_TILE_STAGED4};
+    const int tiles[8] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_CHUNKP, LBMGPU_TILE_ROWCTA, 32, 64, 128,
+                          LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4};
     const int bpss[7] = {1, 2, 3, 4, 5, 6, 8};
     double best = 1e30;
     int btx = b->tile, bbps = b->bps;
