@@ -585,6 +585,8 @@ __device__ void squirmer_update(const Lattice& L, const SqArgs& a) {
 
 template <class S>
 __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const SqArgs a) {
+    pdl_wait();
+    pdl_launch_dependents();
     squirmer_update<S>(L, a);
 }
 

@@ -385,6 +385,8 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
 // ---------------------------------------------------------------------------
 template <class S, int PAR, bool SQ, bool MACRO, bool WR>
 __global__ void __launch_bounds__(256, S::shifted ? 4 : 2) k_bulk(const Lattice L, const StreamArgs a) {
+    pdl_wait();
+    pdl_launch_dependents();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     int y, z;
     if (WR) { y = a.wallrows[2 * blockIdx.y]; z = a.wallrows[2 * blockIdx.y + 1]; }
@@ -441,6 +443,8 @@ __device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a,
 
 template <class S, int PAR, bool SQ, bool MACRO>
 __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
+    pdl_wait();
+    pdl_launch_dependents();
     NodeSums sums;
     zone_cell<S, PAR, SQ, MACRO>(L, a, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums);
     if (MACRO || a.do_mass)

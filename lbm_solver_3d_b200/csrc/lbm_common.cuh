@@ -188,6 +188,15 @@ struct StreamArgs {
 // ---- ensembles (k_batch.cuh) -------------------------------------------------
 constexpr int BATCH_MAX_NX = 256;   // longest x-row of an ensemble member
 
+// Programmatic dependent launch. A kernel launched with programmatic stream
+// serialisation may start before its predecessor in the stream has finished;
+// pdl_wait() blocks until that predecessor has completed and its writes are
+// visible, so it comes before the first read of anything the predecessor
+// writes. pdl_launch_dependents() lets the successor start early. Both are
+// no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 struct RowRef {
     int m, y, z;       // member, row coordinates
     int part;          // entry of the row's partial sums (member base + y + ny*z)

@@ -15,13 +15,32 @@ template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
     k_bulk<S, PAR, SQ, MACRO, false><<<g.grid, g.block, 0, st>>>(L, a);
 }
+// Launch with programmatic stream serialisation: the kernel may be scheduled
+// while its predecessor in the stream finishes, and waits for it in pdl_wait().
+// Used on the stream of the chain wall rows -> zone -> squirmer update, whose
+// kernels follow one another step after step.
+template <class... KArgs, class... Args>
+static void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <class S, int PAR, bool SQ, bool MACRO>
 static void wallrows_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
-    if (g.nwallrows) k_bulk<S, PAR, SQ, MACRO, true><<<dim3(g.grid.x, g.nwallrows, 1), g.block, 0, st>>>(L, a);
+    if (g.nwallrows) launch_pdl(k_bulk<S, PAR, SQ, MACRO, true>, dim3(g.grid.x, g.nwallrows, 1), g.block, 0, st, L, a);
 }
 template <class S, int PAR, bool SQ, bool MACRO>
 static void zone_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
-    if (g.bgrid) k_zone<S, PAR, SQ, MACRO><<<g.bgrid, BOUNDARY_BLOCK, 0, st>>>(L, a);
+    if (g.bgrid) launch_pdl(k_zone<S, PAR, SQ, MACRO>, dim3(g.bgrid), dim3(BOUNDARY_BLOCK), 0, st, L, a);
 }
 
 #define LBMGPU_DISPATCH(FN)                                                                                  \
@@ -48,7 +67,7 @@ inline size_t squirmer_smem() { return sizeof(ChgSh) * SQ_BATCH; }
 
 template <class S>
 static void squirmer_launch(const Lattice& L, const SqArgs& a, cudaStream_t st) {
-    k_squirmer<S><<<1, SQ_THREADS, squirmer_smem(), st>>>(L, a);
+    launch_pdl(k_squirmer<S>, dim3(1), dim3(SQ_THREADS), squirmer_smem(), st, L, a);
 }
 
 template <class S>
