@@ -43,15 +43,16 @@ def mirror(x: np.ndarray, y: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     return xm, ym
 
 
-def dataset_from_npz(path, transient: int = 2000):
-    """Per-member Params-like table, and the (inputs, targets, member) arrays."""
+def dataset_from_npz(path, transient: int = 2000, window: int = 0):
+    """Per-member Params-like table, and the (inputs, targets, member) arrays
+    (window: see surrogate_data.samples)."""
     d = np.load(path)
     table, traj, counts = d["members"], d["traj"], d["counts"]
     off = np.concatenate([[0], np.cumsum(counts)])
     xs, ys, mem = [], [], []
     for i, row in enumerate(table):
         p = member_params(row)
-        x, y = samples(traj[off[i]:off[i + 1]], p, transient)
+        x, y = samples(traj[off[i]:off[i + 1]], p, transient, window)
         xs.append(x); ys.append(y); mem.append(np.full(len(x), i))
     rows = [traj[off[i]:off[i + 1]] for i in range(len(table))]
     return table, rows, np.concatenate(xs), np.concatenate(ys), np.concatenate(mem)

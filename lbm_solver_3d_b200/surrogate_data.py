@@ -53,15 +53,32 @@ def run_ensemble_rows(ps: list[Params], steps: int, chunk: int = 10000, autotune
     return [np.concatenate(r, 0) if r else np.zeros((0, TRAJ_COLS)) for r in rows]
 
 
-def samples(rows: np.ndarray, p: Params, transient: int) -> tuple[np.ndarray, np.ndarray]:
-    """(inputs, targets) of one member's trajectory rows."""
+def samples(rows: np.ndarray, p: Params, transient: int, window: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """(inputs, targets) of one member's trajectory rows.
+
+    window = 0: the instantaneous velocities of the rows. window = k > 0: the
+    velocities from central differences of position and orientation angle over
+    +-k rows, i.e. the drift over 2k * traj_every steps. These no longer carry
+    the step-to-step kicks of nodes being covered and uncovered, which do not
+    move the swimmer on average; the first and last k rows are dropped."""
     r = rows[rows[:, 0] >= transient]
     a, H = p.R, p.NY - 2.0
     U0 = 2.0 * p.B1 / 3.0
-    x = np.stack([(r[:, 2] - 0.5) / a, np.arctan2(r[:, 5], r[:, 4]), np.full(len(r), p.beta),
-                  np.full(len(r), H / a)], 1)
-    y = np.stack([r[:, 7] / U0, r[:, 8] / U0, r[:, 12] * a / U0], 1)
-    return x, y
+    th = np.arctan2(r[:, 5], r[:, 4])
+    x = np.stack([(r[:, 2] - 0.5) / a, th, np.full(len(r), p.beta), np.full(len(r), H / a)], 1)
+    if window <= 0:
+        y = np.stack([r[:, 7] / U0, r[:, 8] / U0, r[:, 12] * a / U0], 1)
+        return x, y
+    k = window
+    if len(r) <= 2 * k:
+        return x[:0], np.zeros((0, 3))
+    dt = r[2 * k:, 0] - r[:-2 * k, 0]
+    thu = np.unwrap(th)
+    ux = (r[2 * k:, 1] - r[:-2 * k, 1]) / dt
+    uy = (r[2 * k:, 2] - r[:-2 * k, 2]) / dt
+    wz = (thu[2 * k:] - thu[:-2 * k]) / dt
+    y = np.stack([ux / U0, uy / U0, wz * a / U0], 1)
+    return x[k:-k], y
 
 
 def build(ps: list[Params], trajs: list[np.ndarray], transient: int):

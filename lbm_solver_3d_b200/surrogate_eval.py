@@ -72,16 +72,19 @@ def main():
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--nets", type=int, default=3)
     ap.add_argument("--fp32", action="store_true", help="FP32 GEMMs instead of BF16")
+    ap.add_argument("--window", type=int, default=0,
+                    help="train on velocities from central differences over +-window rows (0: instantaneous)")
+    ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     d = Path(args.data)
-    table, rows, x, y, mem = dataset_from_npz(d / "surrogate_train.npz", args.transient)
+    table, rows, x, y, mem = dataset_from_npz(d / "surrogate_train.npz", args.transient, args.window)
     # validation: 10% of the training members
     rng = np.random.default_rng(0)
     val_members = rng.choice(len(table), max(1, len(table) // 10), replace=False)
     vmask = np.isin(mem, val_members)
     t0 = time.time()
     s = Surrogate.fit(x[~vmask], y[~vmask], x[vmask], y[vmask], n_nets=args.nets, bf16=not args.fp32,
-                      epochs=args.epochs)
+                      epochs=args.epochs, seed=args.seed)
     t_fit = time.time() - t0
     htable, hrows, hx, hy, hmem = dataset_from_npz(d / "surrogate_heldout.npz", args.transient)
     pred, spread = s.predict(hx)
@@ -100,6 +103,7 @@ def main():
     report = {
         "samples_train": int((~vmask).sum()) * 2, "samples_val": int(vmask.sum()),
         "samples_heldout": int(len(hx)), "gemm": "fp32" if args.fp32 else "bf16", "nets": args.nets,
+        "window": args.window,
         "epochs": args.epochs, "fit_seconds": t_fit,
         "val_loss_final": [lg.val_loss[-1] for lg in s.logs],
         "heldout_instantaneous_velocity_rel_err": {"median": float(np.median(inst)), "mean": float(inst.mean()),
