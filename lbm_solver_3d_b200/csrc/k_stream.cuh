@@ -179,6 +179,49 @@ struct GlobalSrc {
     }
 };
 
+// Collide and push of a node with only fluid neighbours, FP32 arithmetic on
+// stored deviations: the rest population, then one opposite pair (i, i+1) at a
+// time (f+, feq+ and S+ shared by the pair, the odd parts with opposite
+// signs). FORCE = false drops the Guo source terms, which vanish for F = 0.
+template <class S, int PAR, bool FORCE>
+__device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
+                                            const Nbr& nb, const float* d, float dr, float rho, float u, float v,
+                                            float wz, float uF, float k15, bool do_mass, NodeSums& out) {
+    const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
+    {   // rest population: c = 0
+        const float eP = WF(0) * (dr - rho * k15);
+        const float o0 = FORCE ? d[0] - omP * (d[0] - eP) - gP * WF(0) * 3.0f * uF : d[0] - omP * (d[0] - eP);
+        S::st(f + n, o0);
+        if (do_mass) out.mass += (double)S::rt(o0);
+    }
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+        const int io = i + 1;
+        const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+        const float w = WF(i);
+        const float eP = w * (dr + rho * (4.5f * cu * cu - k15));  // feq+ - w
+        const float eM = 3.0f * w * rho * cu;                       // feq-
+        const float fP = 0.5f * (d[i] + d[io]), fM = 0.5f * (d[i] - d[io]);
+        float A, B;
+        if (FORCE) {
+            A = gP * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - omP * (fP - eP);
+            B = L.cm[i] - omM * (fM - eM);
+        } else {
+            A = -omP * (fP - eP);
+            B = -omM * (fM - eM);
+        }
+        const float oi = d[i] + A + B, oo = d[io] + A - B;
+        if (PAR == 0) {
+            S::st(f + (size_t)io * N + n, oi);
+            S::st(f + (size_t)i * N + n, oo);
+        } else {
+            S::st(f + (size_t)i * N + nb.of(n, i), oi);
+            S::st(f + (size_t)io * N + nb.of(n, io), oo);
+        }
+        if (do_mass) out.mass += (double)S::rt(oi) + (double)S::rt(oo);
+    }
+}
+
 template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
                                             uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
@@ -287,32 +330,10 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
         const float k15 = 1.5f * usq;
         if (!boundary) {
-            {   // rest population: c = 0
-                const float eP = WF(0) * (dr - rho * k15);
-                const float o0 = d[0] - omP * (d[0] - eP) - gP * WF(0) * 3.0f * uF;
-                S::st(f + n, o0);
-                if (do_mass) out.mass += (double)S::rt(o0);
-            }
-#pragma unroll
-            for (int i = 1; i < Q; i += 2) {
-                const int io = i + 1;
-                const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-                const float w = WF(i);
-                const float eP = w * (dr + rho * (4.5f * cu * cu - k15));  // feq+ - w
-                const float eM = 3.0f * w * rho * cu;                       // feq-
-                const float fP = 0.5f * (d[i] + d[io]), fM = 0.5f * (d[i] - d[io]);
-                const float A = gP * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - omP * (fP - eP);
-                const float B = L.cm[i] - omM * (fM - eM);
-                const float oi = d[i] + A + B, oo = d[io] + A - B;
-                if (PAR == 0) {
-                    S::st(f + (size_t)io * N + n, oi);
-                    S::st(f + (size_t)i * N + n, oo);
-                } else {
-                    S::st(f + (size_t)i * N + nb.of(n, i), oi);
-                    S::st(f + (size_t)io * N + nb.of(n, io), oo);
-                }
-                if (do_mass) out.mass += (double)S::rt(oi) + (double)S::rt(oo);
-            }
+            if (L.force_free)   // uniform: the Guo source terms are exactly zero
+                plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, rho, u, v, wz, uF, k15, do_mass, out);
+            else
+                plain_pairs<S, PAR, true>(L, f, N, n, nb, d, dr, rho, u, v, wz, uF, k15, do_mass, out);
         } else {
             float post[Q];
             post[0] = d[0] - omP * (d[0] - WF(0) * (dr - rho * k15)) - gP * WF(0) * 3.0f * uF;

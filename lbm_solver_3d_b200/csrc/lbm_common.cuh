@@ -85,6 +85,7 @@ struct Lattice {
     // cF[i] = c_i . F and cm[i] = gM * 3 w_i (c_i . F) for the odd i of each pair
     float omPf, omMf, gPf, gMf, Ff[3], uFh[3];
     float cF[Q], cm[Q];
+    int force_free;        // F = 0: the Guo source terms vanish (FP32 arithmetic skips them)
 };
 
 // ---- the zone around the sphere ----------------------------------------------

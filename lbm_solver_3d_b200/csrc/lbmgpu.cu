@@ -603,6 +603,7 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     L.F[0] = p->fx; L.F[1] = p->fy; L.F[2] = p->fz;
     L.omPf = (float)L.omP; L.omMf = (float)L.omM; L.gPf = (float)L.gP; L.gMf = (float)L.gM;
     for (int d = 0; d < 3; ++d) { L.Ff[d] = (float)L.F[d]; L.uFh[d] = 0.0f; }
+    L.force_free = L.F[0] == 0.0 && L.F[1] == 0.0 && L.F[2] == 0.0;
     for (int i = 0; i < Q; ++i) {
         const double cF = CX(i) * L.F[0] + CY(i) * L.F[1] + CZ(i) * L.F[2];
         L.cF[i] = (float)cF;
