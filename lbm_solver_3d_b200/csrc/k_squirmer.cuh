@@ -37,6 +37,7 @@ namespace lbmgpu {
 
 constexpr int SQ_THREADS = 512;
 constexpr int SQ_BATCH = 256;
+constexpr int SQ_SORT_CAP = 2048;   // changes ordered in shared memory (3 ints each)
 constexpr int STAGE_BODY = 1, STAGE_REMAP = 2, STAGE_LOOP = 4, STAGE_FORCE = 8;
 
 struct SqArgs {
@@ -59,6 +60,8 @@ struct SqArgs {
     int* cand;                // candidate nodes of the remap / link scans (chg_cap)
     uint8_t* mark;            // chg_cap bytes: one verdict per candidate
     int chg_cap;
+    int* shell;               // cached remap candidates (chg_cap entries)
+    ShellCache* shell_hdr;
     double* traj;             // TRAJ_RING x TRAJ_COLS
     SqState* sq;
     int parity;               // parity of the state being remapped
@@ -127,27 +130,32 @@ struct AxisRange {
     __device__ int at(int b) const { return b < wrap ? b : start + (b - wrap); }
 };
 
+static_assert(3 * SQ_SORT_CAP * sizeof(int) <= SQ_BATCH * sizeof(ChgSh), "the change sort fits the batch stage");
+
 template <class S>
 __device__ void squirmer_update(const Lattice& L, const SqArgs& a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ChgSh* ch = reinterpret_cast<ChgSh*>(smem_raw);
     __shared__ SqState s;
     __shared__ double sums[8];
-    __shared__ int sh_total, sh_box[6], sh_skip;
+    __shared__ int sh_total, sh_box[6], sh_rebuild, sh_ncand;
     __shared__ double sh_mass_delta;
     __shared__ long long sh_dfluid;
     typedef cub::BlockScan<int, SQ_THREADS> Scan;
     __shared__ typename Scan::TempStorage scan_tmp;
 
     const int tid = threadIdx.x;
+    {   // the state, one word per thread
+        constexpr int NS = (int)(sizeof(SqState) / 4);
+        static_assert(sizeof(SqState) % 4 == 0 && NS <= SQ_THREADS, "one word per thread");
+        if (tid < NS) reinterpret_cast<uint32_t*>(&s)[tid] = reinterpret_cast<const uint32_t*>(a.sq)[tid];
+    }
     if (tid == 0) {
-        s = *a.sq;
-        sh_skip = (s.status & (ST_NAN | ST_REMAP_RANGE | ST_LINK_OVERFLOW)) != 0;
         sh_mass_delta = 0.0;
         sh_dfluid = 0;
     }
     __syncthreads();
-    if (sh_skip) return;  // the state is already invalid; the host reports it
+    if (s.status & (ST_NAN | ST_REMAP_RANGE | ST_LINK_OVERFLOW)) return;  // invalid already; the host reports it
 
     const long long t_now = s.t + 1;
     const bool loop = (a.stages & STAGE_LOOP) != 0;
@@ -247,84 +255,143 @@ __device__ void squirmer_update(const Lattice& L, const SqArgs& a) {
         // Only nodes within one cell of the sphere's surface can change: the
         // centre moved less than a cell since the last remap (checked in stage
         // BODY), so nodes deeper than that were and stay PARTICLE and nodes
-        // farther out were and stay FLUID. The filter is conservative (slack
-        // 0.05); the decision itself uses the reference's exact offset.
-        const double Rin = fmax(s.R - 1.05, 0.0), Rout = s.R + 1.05;
-        const double Rin2 = Rin * Rin, Rout2 = Rout * Rout;
+        // farther out were and stay FLUID. The candidates are the nodes within
+        // R +- 1.05 of the centre (0.05 covers the cheap distance against the
+        // reference's exact offset, which makes the decision). The shell list
+        // widens that by SHELL_SLACK around a reference centre, so it holds
+        // every candidate while the centre stays within SHELL_SLACK of it
+        // (triangle inequality), and the box walk that builds it runs only
+        // when the centre leaves that ball.
 
-        // (1) candidates, compacted in box order (z, y, x of the first visit)
-        const int chunk = (V + SQ_THREADS - 1) / SQ_THREADS;
-        const int k0 = min(V, tid * chunk), k1 = min(V, k0 + chunk);
-        auto box_walk = [&](auto&& visit) {
-            if (k0 >= k1) return;
-            int bx = k0 % bw, by = (k0 / bw) % bh, bz = k0 / (bw * bh);
-            int x = (((bx0 + bx) % L.nx) + L.nx) % L.nx;
-            int y = (((by0 + by) % L.ny) + L.ny) % L.ny;
-            int z = (((bz0 + bz) % L.nz) + L.nz) % L.nz;
-            for (int k = k0; k < k1; ++k) {
-                // a box wider than the lattice revisits nodes; the first visit counts
-                if (bx < L.nx && by < L.ny && bz < L.nz) visit(k, x, y, z);
-                if (++bx == bw) {
-                    bx = 0; x = (((bx0) % L.nx) + L.nx) % L.nx;
-                    if (++by == bh) { by = 0; y = (((by0) % L.ny) + L.ny) % L.ny; ++bz; if (++z == L.nz) z = 0; }
-                    else if (++y == L.ny) y = 0;
-                } else if (++x == L.nx) x = 0;
+        // (1) candidates: the cached shell, rebuilt in box order (z, y, x of
+        // the first visit) when the centre has left the slack around the
+        // reference centre of the list. A cached list that yields more than
+        // SQ_SORT_CAP changes is rebuilt at once (second pass).
+        if (tid == 0) {
+            const ShellCache hc = *a.shell_hdr;
+            const double d0 = s.X[0] - hc.X[0], d1 = s.X[1] - hc.X[1], d2 = s.X[2] - hc.X[2];
+            sh_rebuild = !(hc.valid && d0 * d0 + d1 * d1 + d2 * d2 < SHELL_SLACK * SHELL_SLACK);
+            sh_ncand = hc.n;
+        }
+        __syncthreads();
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {
+                if (!(!sh_rebuild && sh_total > SQ_SORT_CAP)) break;   // uniform
+                __syncthreads();
+                if (tid == 0) sh_rebuild = 1;
+                __syncthreads();
             }
-        };
-        {
-            int cnt = 0;
-            box_walk([&](int, int x, int y, int z) {
-                const double r2 = approx_r2(x, y, z);
-                cnt += (r2 >= Rin2 && r2 < Rout2);
-            });
-            int off = 0;
-            Scan(scan_tmp).ExclusiveSum(cnt, off, sh_total);
+            const int chunk = (V + SQ_THREADS - 1) / SQ_THREADS;
+            const int k0 = min(V, tid * chunk), k1 = min(V, k0 + chunk);
+            auto box_walk = [&](auto&& visit) {
+                if (k0 >= k1) return;
+                int bx = k0 % bw, by = (k0 / bw) % bh, bz = k0 / (bw * bh);
+                int x = (((bx0 + bx) % L.nx) + L.nx) % L.nx;
+                int y = (((by0 + by) % L.ny) + L.ny) % L.ny;
+                int z = (((bz0 + bz) % L.nz) + L.nz) % L.nz;
+                for (int k = k0; k < k1; ++k) {
+                    // a box wider than the lattice revisits nodes; the first visit counts
+                    if (bx < L.nx && by < L.ny && bz < L.nz) visit(k, x, y, z);
+                    if (++bx == bw) {
+                        bx = 0; x = (((bx0) % L.nx) + L.nx) % L.nx;
+                        if (++by == bh) { by = 0; y = (((by0) % L.ny) + L.ny) % L.ny; ++bz; if (++z == L.nz) z = 0; }
+                        else if (++y == L.ny) y = 0;
+                    } else if (++x == L.nx) x = 0;
+                }
+            };
+            if (sh_rebuild) {   // uniform
+                const double Sin = fmax(s.R - 1.05 - SHELL_SLACK, 0.0), Sout = s.R + 1.05 + SHELL_SLACK;
+                const double Sin2 = Sin * Sin, Sout2 = Sout * Sout;
+                int cnt = 0;
+                box_walk([&](int, int x, int y, int z) {
+                    const double r2 = approx_r2(x, y, z);
+                    cnt += (r2 >= Sin2 && r2 < Sout2);
+                });
+                int off = 0;
+                Scan(scan_tmp).ExclusiveSum(cnt, off, sh_total);
+                __syncthreads();
+                box_walk([&](int, int x, int y, int z) {
+                    const double r2 = approx_r2(x, y, z);
+                    if (r2 >= Sin2 && r2 < Sout2) {
+                        if (off < a.chg_cap) a.shell[off] = x + L.nx * (y + L.ny * z);
+                        ++off;
+                    }
+                });
+                if (tid == 0) {
+                    sh_ncand = min(sh_total, a.chg_cap);
+                    ShellCache hc;
+                    for (int d = 0; d < 3; ++d) hc.X[d] = s.X[d];
+                    hc.n = sh_ncand;
+                    hc.valid = 1;
+                    *a.shell_hdr = hc;
+                }
+                __syncthreads();
+            }
+            const int ncand = sh_ncand;
+            // (2) exact test of each candidate (flag load + the reference's offset)
+            for (int c = tid; c < ncand; c += SQ_THREADS) {
+                const unsigned n = (unsigned)a.shell[c];
+                uint8_t mk = 0;
+                const uint8_t ty = a.flag[n] & TYPE_MASK;
+                if (ty != T_WALL) {
+                    const int x = (int)(n % (unsigned)L.nx), y = (int)((n / (unsigned)L.nx) % (unsigned)L.ny),
+                              z = (int)(n / L.nxy);
+                    double r[3];
+                    offset_from_squirmer(L, &s, x, y, z, r);
+                    const bool inside = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < R2;
+                    if (inside != (ty == T_PARTICLE)) mk = inside ? 1 : 2;
+                }
+                a.mark[c] = mk;
+            }
             __syncthreads();
-            box_walk([&](int, int x, int y, int z) {
-                const double r2 = approx_r2(x, y, z);
-                if (r2 >= Rin2 && r2 < Rout2) {
-                    if (off < a.chg_cap)
-                        a.cand[off] = x + L.nx * (y + L.ny * z);
+            // (3) changed nodes in list order
+            {
+                const int ch2 = (ncand + SQ_THREADS - 1) / SQ_THREADS;
+                const int c0 = min(ncand, tid * ch2), c1 = min(ncand, c0 + ch2);
+                int cnt = 0;
+                for (int c = c0; c < c1; ++c) cnt += a.mark[c] != 0;
+                int off = 0;
+                Scan(scan_tmp).ExclusiveSum(cnt, off, sh_total);
+                __syncthreads();
+                for (int c = c0; c < c1; ++c) {
+                    const uint8_t mk = a.mark[c];
+                    if (!mk) continue;
+                    a.chg_node[off] = a.shell[c];
+                    a.chg_key[off] = mk;
                     ++off;
                 }
-            });
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        const int ncand = min(sh_total, a.chg_cap);
-        // (2) exact test of each candidate (flag load + the reference's offset)
-        for (int c = tid; c < ncand; c += SQ_THREADS) {
-            const unsigned n = (unsigned)a.cand[c];
-            uint8_t mk = 0;
-            const uint8_t ty = a.flag[n] & TYPE_MASK;
-            if (ty != T_WALL) {
+        // A list cached under an earlier box is in that box's order: put the
+        // changes in the order of their first visit in this box (rank sort on
+        // the visit index; distinct nodes have distinct indices).
+        if (!sh_rebuild && sh_total > 1) {   // uniform
+            const int nchg = sh_total;
+            int* keys = reinterpret_cast<int*>(smem_raw);
+            int* nodes = keys + SQ_SORT_CAP;
+            int* kinds = nodes + SQ_SORT_CAP;
+            for (int e = tid; e < nchg; e += SQ_THREADS) {
+                const unsigned n = (unsigned)a.chg_node[e];
                 const int x = (int)(n % (unsigned)L.nx), y = (int)((n / (unsigned)L.nx) % (unsigned)L.ny),
                           z = (int)(n / L.nxy);
-                double r[3];
-                offset_from_squirmer(L, &s, x, y, z, r);
-                const bool inside = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < R2;
-                if (inside != (ty == T_PARTICLE)) mk = inside ? 1 : 2;
+                const int kx = ((x - bx0) % L.nx + L.nx) % L.nx;
+                const int ky = ((y - by0) % L.ny + L.ny) % L.ny;
+                const int kz = ((z - bz0) % L.nz + L.nz) % L.nz;
+                keys[e] = (kz * bh + ky) * bw + kx;
+                nodes[e] = (int)n;
+                kinds[e] = a.chg_key[e];
             }
-            a.mark[c] = mk;
-        }
-        __syncthreads();
-        // (3) changed nodes in box order
-        {
-            const int ch2 = (ncand + SQ_THREADS - 1) / SQ_THREADS;
-            const int c0 = min(ncand, tid * ch2), c1 = min(ncand, c0 + ch2);
-            int cnt = 0;
-            for (int c = c0; c < c1; ++c) cnt += a.mark[c] != 0;
-            int off = 0;
-            Scan(scan_tmp).ExclusiveSum(cnt, off, sh_total);
             __syncthreads();
-            for (int c = c0; c < c1; ++c) {
-                const uint8_t mk = a.mark[c];
-                if (!mk) continue;
-                a.chg_node[off] = a.cand[c];
-                a.chg_key[off] = mk;
-                ++off;
+            for (int e = tid; e < nchg; e += SQ_THREADS) {
+                const int ke = keys[e];
+                int rank = 0;
+                for (int j = 0; j < nchg; ++j) rank += keys[j] < ke;
+                a.chg_node[rank] = nodes[e];
+                a.chg_key[rank] = kinds[e];
             }
+            __syncthreads();
         }
-        __syncthreads();
         const int total = sh_total;
         for (int k = tid; k < total; k += SQ_THREADS) a.ordermap[a.chg_node[k]] = k;
         __syncthreads();
@@ -594,13 +661,22 @@ __global__ void __launch_bounds__(SQ_THREADS) k_squirmer(const Lattice L, const 
 // per-step settings are the same for all members.
 template <class S>
 __global__ void __launch_bounds__(SQ_THREADS) k_squirmer_batch(const Lattice* lat, const SqArgs* args, SqStep st) {
-    __shared__ Lattice L;
-    __shared__ SqArgs A;
-    if (threadIdx.x == 0) {
-        L = lat[blockIdx.x];
-        A = args[blockIdx.x];
-        A.parity = st.parity; A.stages = st.stages; A.corr_step = st.corr_step;
-        A.zslot_a = st.zslot_a; A.zslot_b = st.zslot_b;
+    __shared__ __align__(16) Lattice L;
+    __shared__ __align__(16) SqArgs A;
+    {   // the member's records, one word per thread, with this step's settings
+        constexpr int NL = (int)(sizeof(Lattice) / 4), NA = (int)(sizeof(SqArgs) / 4);
+        static_assert(NL <= SQ_THREADS && NA <= SQ_THREADS, "one word per thread");
+        const int t = threadIdx.x;
+        if (t < NL) reinterpret_cast<uint32_t*>(&L)[t] = reinterpret_cast<const uint32_t*>(lat + blockIdx.x)[t];
+        if (t < NA) {
+            uint32_t w = reinterpret_cast<const uint32_t*>(args + blockIdx.x)[t];
+            if (t == (int)(offsetof(SqArgs, parity) / 4)) w = (uint32_t)st.parity;
+            if (t == (int)(offsetof(SqArgs, stages) / 4)) w = (uint32_t)st.stages;
+            if (t == (int)(offsetof(SqArgs, corr_step) / 4)) w = (uint32_t)st.corr_step;
+            if (t == (int)(offsetof(SqArgs, zslot_a) / 4)) w = (uint32_t)st.zslot_a;
+            if (t == (int)(offsetof(SqArgs, zslot_b) / 4)) w = (uint32_t)st.zslot_b;
+            reinterpret_cast<uint32_t*>(&A)[t] = w;
+        }
     }
     __syncthreads();
     squirmer_update<S>(L, A);

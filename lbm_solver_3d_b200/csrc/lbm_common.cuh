@@ -157,6 +157,17 @@ struct SqState {
     int status;
 };
 
+// The shell of remap candidates (nodes whose distance to a reference centre
+// is within R +- (1.05 + SHELL_SLACK)), kept between squirmer updates. While
+// the centre stays within SHELL_SLACK of the reference centre, every node that
+// can change type lies in it.
+struct ShellCache {
+    double X[3];   // reference centre (unwrapped, like SqState::X)
+    int n;         // candidates in the list
+    int valid;     // 0: rebuild on the next remap
+};
+constexpr double SHELL_SLACK = 0.75;
+
 constexpr int TRAJ_RING = 4096;
 constexpr int TRAJ_COLS = 15;
 

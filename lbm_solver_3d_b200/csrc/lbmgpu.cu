@@ -79,6 +79,8 @@ struct lbmgpu_handle {
     int* chg_node = nullptr;
     int* chg_key = nullptr;
     int* cand = nullptr;
+    int* shell = nullptr;          // cached remap candidates
+    ShellCache* shell_hdr = nullptr;
     uint8_t* mark = nullptr;
     int chg_cap = 0;
     double* traj = nullptr;
@@ -166,7 +168,7 @@ SqArgs squirmer_args(lbmgpu_handle* h, int parity, int stages, int corr_step, in
     a.block_part_b = h->block_part_b; a.nblocks_b = (int)h->nblocks_b;
     a.block_part_w = nullptr; a.nblocks_w = 0;
     a.ordermap = h->ordermap; a.chg_node = h->chg_node; a.chg_key = h->chg_key; a.cand = h->cand; a.mark = h->mark;
-    a.chg_cap = h->chg_cap;
+    a.chg_cap = h->chg_cap; a.shell = h->shell; a.shell_hdr = h->shell_hdr;
     a.traj = h->traj; a.sq = h->sq; a.parity = parity; a.stages = stages;
     a.corr_step = corr_step; a.zslot_a = za; a.zslot_b = zb;
     return a;
@@ -407,7 +409,7 @@ void free_all(lbmgpu_handle* h) {
     if (h->member) { h->f = nullptr; h->flag = nullptr; }
     void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wallrows, h->links, h->linkslot,
                     h->link_part, h->block_part, h->block_part_b, h->ordermap, h->chg_node, h->chg_key,
-                    h->cand, h->mark, h->traj, h->sq, h->scratch, h->small};
+                    h->cand, h->mark, h->traj, h->sq, h->scratch, h->small, h->shell, h->shell_hdr};
     for (void* q : ptrs) if (q) cudaFree(q);
     for (cudaEvent_t e : {h->ev_b[0], h->ev_b[1], h->ev_z, h->ev_s, h->ev_fork, h->ev_join})
         if (e) cudaEventDestroy(e);
@@ -665,6 +667,8 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
         CTRY(cudaMalloc(&h->chg_key, (size_t)h->chg_cap * sizeof(int)));
         CTRY(cudaMalloc(&h->mark, (size_t)h->chg_cap));
         CTRY(cudaMalloc(&h->cand, (size_t)h->chg_cap * sizeof(int)));
+        CTRY(cudaMalloc(&h->shell, (size_t)h->chg_cap * sizeof(int)));
+        CTRY(cudaMalloc(&h->shell_hdr, sizeof(ShellCache)));
         CTRY(cudaMalloc(&h->traj, (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double)));
     }
     cudaStream_t st = h->stream;
@@ -683,6 +687,7 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     CTRY(cudaMemcpyAsync(h->flag, hi.flag.data(), N, cudaMemcpyHostToDevice, st));
     if (h->has_sq) {
         k_fill_i<<<592, 256, 0, st>>>(h->ordermap, N, -1);
+        CTRY(cudaMemsetAsync(h->shell_hdr, 0, sizeof(ShellCache), st));   // no shell yet
         CTRY(cudaMemsetAsync(h->linkslot, 0, N * sizeof(int), st));
         if (!hi.links.empty()) {
             CTRY(cudaMemcpyAsync(h->links, hi.links.data(), hi.links.size() * sizeof(int), cudaMemcpyHostToDevice, st));
