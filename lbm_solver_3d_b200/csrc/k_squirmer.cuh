@@ -37,7 +37,8 @@ namespace lbmgpu {
 
 constexpr int SQ_THREADS = 512;
 constexpr int SQ_BATCH = 256;
-constexpr int SQ_SORT_CAP = 2048;   // changes ordered in shared memory (3 ints each)
+constexpr int SQ_SORT_CAP = 2048;
+constexpr int SQ_GROUP = 4;         // remap candidates tested per thread with their loads in flight together   // changes ordered in shared memory (3 ints each)
 constexpr int STAGE_BODY = 1, STAGE_REMAP = 2, STAGE_LOOP = 4, STAGE_FORCE = 8;
 
 struct SqArgs {
@@ -328,20 +329,36 @@ __device__ void squirmer_update(const Lattice& L, const SqArgs& a) {
                 __syncthreads();
             }
             const int ncand = sh_ncand;
-            // (2) exact test of each candidate (flag load + the reference's offset)
-            for (int c = tid; c < ncand; c += SQ_THREADS) {
-                const unsigned n = (unsigned)a.shell[c];
-                uint8_t mk = 0;
-                const uint8_t ty = a.flag[n] & TYPE_MASK;
-                if (ty != T_WALL) {
-                    const int x = (int)(n % (unsigned)L.nx), y = (int)((n / (unsigned)L.nx) % (unsigned)L.ny),
-                              z = (int)(n / L.nxy);
-                    double r[3];
-                    offset_from_squirmer(L, &s, x, y, z, r);
-                    const bool inside = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < R2;
-                    if (inside != (ty == T_PARTICLE)) mk = inside ? 1 : 2;
+            // (2) exact test of each candidate (flag load + the reference's
+            // offset), SQ_GROUP candidates per thread at a time: their node
+            // indices and flags are all loaded before the first test
+            for (int c0 = tid; c0 < ncand; c0 += SQ_GROUP * SQ_THREADS) {
+                unsigned nn[SQ_GROUP];
+                uint8_t ty[SQ_GROUP];
+#pragma unroll
+                for (int g = 0; g < SQ_GROUP; ++g) {
+                    const int c = c0 + g * SQ_THREADS;
+                    nn[g] = c < ncand ? (unsigned)a.shell[c] : 0u;
                 }
-                a.mark[c] = mk;
+#pragma unroll
+                for (int g = 0; g < SQ_GROUP; ++g)
+                    ty[g] = c0 + g * SQ_THREADS < ncand ? (uint8_t)(a.flag[nn[g]] & TYPE_MASK) : (uint8_t)T_WALL;
+#pragma unroll
+                for (int g = 0; g < SQ_GROUP; ++g) {
+                    const int c = c0 + g * SQ_THREADS;
+                    if (c >= ncand) break;
+                    const unsigned n = nn[g];
+                    uint8_t mk = 0;
+                    if (ty[g] != T_WALL) {
+                        const int x = (int)(n % (unsigned)L.nx), y = (int)((n / (unsigned)L.nx) % (unsigned)L.ny),
+                                  z = (int)(n / L.nxy);
+                        double r[3];
+                        offset_from_squirmer(L, &s, x, y, z, r);
+                        const bool inside = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < R2;
+                        if (inside != (ty[g] == T_PARTICLE)) mk = inside ? 1 : 2;
+                    }
+                    a.mark[c] = mk;
+                }
             }
             __syncthreads();
             // (3) changed nodes in list order

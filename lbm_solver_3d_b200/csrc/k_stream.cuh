@@ -168,6 +168,16 @@ __device__ __forceinline__ bool wall_dir(int i, uint8_t wr) {
     return (CY(i) < 0 && (wr & 1)) || (CY(i) > 0 && (wr & 2)) || (CZ(i) < 0 && (wr & 4)) || (CZ(i) > 0 && (wr & 8));
 }
 
+// Types of the 18 neighbours n + c_i, 2 bits each at bit 2i (the loads are
+// independent and go out together).
+__device__ __forceinline__ uint64_t neighbour_types(const Lattice& L, const uint8_t* __restrict__ flag, unsigned n,
+                                                    const Nbr& nb) {
+    uint64_t m = 0;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) m |= (uint64_t)(flag[nb.of(n, i)] & TYPE_MASK) << (2 * i);
+    return m;
+}
+
 // Where update_node reads the 19 logical populations from: the population
 // array itself (GlobalSrc), or a copy staged in shared memory (StagedSrc in
 // k_batch.cuh). Either returns the stored values converted by S::ld.
@@ -233,6 +243,10 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
     // GENERAL: neighbour types from the flag bytes; otherwise only whole wall
     // layers next to the row (wallrow) can be solid.
     const bool boundary = GENERAL ? (fl & (NEAR_WALL | NEAR_PARTICLE)) != 0 : wallrow != 0;
+    // GENERAL: the neighbours' types, 2 bits per direction, all read before the
+    // first population store (a byte load may alias the stores, so a load
+    // inside the direction loop would wait for the stores before it)
+    const uint64_t ntypes = GENERAL && boundary ? neighbour_types(L, a.flag, n, nb) : 0ull;
     const SqState* __restrict__ sq = a.sq;
     const bool do_mass = a.do_mass != 0;
 
@@ -274,7 +288,8 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
             T* local = f + (size_t)io * N + n;
             T* remote = f + (size_t)i * N + nbi;
             uint8_t tt = T_FLUID;
-            if (boundary && i != 0) tt = GENERAL ? (a.flag[nbi] & TYPE_MASK) : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
+            if (boundary && i != 0)
+                tt = GENERAL ? (uint8_t)((ntypes >> (2 * i)) & 3u) : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
             if (tt == T_FLUID) {  // push (lbm.cpp:186)
                 S::st(PAR == 0 ? local : remote, fpost);
                 if (do_mass) out.mass += fpost;
@@ -357,7 +372,8 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                 T* local = f + (size_t)OPP(i) * N + n;
                 T* remote = f + (size_t)i * N + nbi;
                 const uint8_t tt = i == 0 ? T_FLUID
-                                   : GENERAL ? (a.flag[nbi] & TYPE_MASK) : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
+                                   : GENERAL ? (uint8_t)((ntypes >> (2 * i)) & 3u)
+                                             : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
                 if (tt == T_FLUID) {
                     S::st(PAR == 0 ? local : remote, dpost);
                     if (do_mass) out.mass += (double)S::rt(dpost);
