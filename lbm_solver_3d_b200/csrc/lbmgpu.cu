@@ -4,7 +4,11 @@
 //  accessors.
 //
 //  Time loop (lbmgpu_run). Step s runs three kernels:
-//    B(s)  k_bulk     every fluid node outside the zone (wall rows included)
+//    B(s)  k_bulk     every fluid node outside the zone (two launches when
+//                     there are walls: the rows next to a wall are a launch
+//                     of their own, on stream b ahead of Z(s), or on stream
+//                     a after the rest of B(s) when the bulk is short and a
+//                     squirmer's chain Z -> S is the longer path)
 //    Z(s)  k_zone     the zone around the sphere
 //    S(s)  k_squirmer rigid body, remap, link list, bookkeeping
 //  on two streams, with exactly the dependencies the data needs:
@@ -93,6 +97,7 @@ struct lbmgpu_handle {
     int zone_cells = 0, zw[3] = {0, 0, 0};
     int period = 6;              // steps after which the launch pattern repeats
     bool corr_in_graph = false;  // correction steps are part of the captured pattern
+    bool wallrows_on_a = false;  // wall rows follow the bulk on stream a (short bulk, squirmer chain)
 
     // host mirrors
     long long t_main = 0;        // time steps issued (AA parity; step s = t_main + 1)
@@ -438,10 +443,11 @@ void issue_fused(lbmgpu_handle* h, cudaStream_t sa, cudaStream_t sb, const StepP
     cudaStreamWaitEvent(sa, h->ev_z, 0);
     if (sp.apply) cudaStreamWaitEvent(sa, h->ev_s, 0);
     h->lz->bulk(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sa);
+    int k = 1;
+    if (h->geom.nwallrows && h->wallrows_on_a) { h->lz->wallrows(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sa); ++k; }
     cudaEventRecord(h->ev_b[sp.s & 1], sa);
     cudaStreamWaitEvent(sb, h->ev_b[(sp.s - 1) & 1], 0);
-    int k = 1;
-    if (h->geom.nwallrows) { h->lz->wallrows(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sb); ++k; }
+    if (h->geom.nwallrows && !h->wallrows_on_a) { h->lz->wallrows(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sb); ++k; }
     if (h->geom.bgrid) { h->lz->zone(par, h->has_sq != 0, sp.macro, h->L, a, h->geom, sb); ++k; }
     cudaEventRecord(h->ev_z, sb);
     if (sp.macro) {
@@ -616,6 +622,12 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     HostInit hi;
     build_initial(*p, hi);
     h->geom.nwallrows = (unsigned)(hi.wallrows.size() / 2);
+    // Wall rows and zone nodes are disjoint and the wall rows need only what
+    // the bulk of the same step needs, so they may go on either stream. On
+    // stream b they overlap the bulk but lengthen the chain wall rows -> zone ->
+    // squirmer; when the bulk moves less than ~200 MB (about 40 us) that chain
+    // is the step, and they go after the bulk on stream a instead.
+    h->wallrows_on_a = h->has_sq && (double)Q * 2.0 * h->esize * (double)N <= 200e6;
     const int box = h->has_sq ? 2 * (int)std::ceil(p->radius) + 8 : 1;
     const long long boxvol = (long long)box * box * box;
     h->link_cap = (int)std::max<long long>(boxvol, (long long)hi.links.size() + 1);
