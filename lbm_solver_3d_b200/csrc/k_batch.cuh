@@ -584,8 +584,12 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone_batch(const Lattice* __
     }
     __syncthreads();
     if ((int)(blockIdx.x * BOUNDARY_BLOCK) >= A.zone_cells) return;  // block-uniform
+    __shared__ __align__(16) SqState zsq;
+    __shared__ LinkStash<S> stash[Q * BOUNDARY_BLOCK];
+    copy_sq_state(&zsq, A.sq);
+    __syncthreads();
     NodeSums sums;
-    zone_cell<S, PAR, true, MACRO>(L, A, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums);
+    zone_cell<S, PAR, true, MACRO>(L, A, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums, &zsq, stash);
     if (MACRO || st.do_mass)
         block_reduce4<BOUNDARY_BLOCK>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass,
                                       zone_part + ((size_t)m * gzmax + blockIdx.x) * BLOCK_PART);

@@ -46,6 +46,9 @@
 //  sign); boundary-link velocities, the momentum exchange and all sums are FP64.
 // ============================================================================
 #pragma once
+#include <type_traits>
+
+#include "k_logical.cuh"
 #include "lbm_common.cuh"
 
 namespace lbmgpu {
@@ -146,7 +149,14 @@ struct NodeSums {
     double fw[3] = {0, 0, 0};
     double mass = 0;
     double fp[3] = {0, 0, 0}, tp[3] = {0, 0, 0};
+    unsigned pmask = 0;   // GENERAL: directions of the node's particle links, left for zone_particle_links
+    double rho = 0;       // GENERAL: the node's density, for zone_particle_links
 };
+
+// Post-collision values of a zone block's particle links, [direction][thread]:
+// the population itself (FP64) or its deviation (shifted forms).
+template <class S>
+using LinkStash = typename std::conditional<S::shifted, float, double>::type;
 
 // ---------------------------------------------------------------------------
 //  update_node: the whole LBM::step body for one fluid node n.
@@ -232,10 +242,13 @@ __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __r
     }
 }
 
+// GENERAL: the particle links are not computed here. Their post-collision
+// values go to link_stash[i * BOUNDARY_BLOCK + threadIdx.x], their directions
+// to out.pmask, and zone_particle_links finishes them with the whole warp.
 template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
                                             uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
-                                            const Src& src = Src()) {
+                                            const Src& src = Src(), LinkStash<S>* link_stash = nullptr) {
     using T = typename S::T;
     T* __restrict__ f = static_cast<T*>(a.f);
     const unsigned N = L.N;
@@ -272,6 +285,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         const double u = (mx + 0.5 * Fx) / r, v = (my + 0.5 * Fy) / r, wz = (mz + 0.5 * Fz) / r;
         if (store_rho) a.rho[n] = r;
         if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
+        if (GENERAL) out.rho = r;
         const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -295,12 +309,13 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                 if (do_mass) out.mass += fpost;
                 continue;
             }
-            // halfway bounce-back with moving-boundary correction (lbm.cpp:189-199)
-            double ub[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
-            if (GENERAL && tt == T_PARTICLE) {
-                offset_from_squirmer(L, sq, x + 0.5 * CX(i), y + 0.5 * CY(i), z + 0.5 * CZ(i), rb);
-                surface_velocity(sq, rb, ub, true);
+            if (GENERAL && tt == T_PARTICLE) {   // finished by zone_particle_links
+                link_stash[i * BOUNDARY_BLOCK + threadIdx.x] = fpost;
+                out.pmask |= 1u << i;
+                continue;
             }
+            // halfway bounce-back at a wall (lbm.cpp:189-199, u_b = 0)
+            const double ub[3] = {0, 0, 0};
             const double cub = CX(i) * ub[0] + CY(i) * ub[1] + CZ(i) * ub[2];
             const double fb = fpost - 6.0 * WD(i) * r * cub;
             S::st(PAR == 0 ? remote : local, fb);
@@ -310,13 +325,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
             const double dpx = sm * CX(i) - dl * ub[0];
             const double dpy = sm * CY(i) - dl * ub[1];
             const double dpz = sm * CZ(i) - dl * ub[2];
-            if (tt == T_WALL) { out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz; }
-            else {
-                out.fp[0] += dpx; out.fp[1] += dpy; out.fp[2] += dpz;
-                out.tp[0] += rb[1] * dpz - rb[2] * dpy;
-                out.tp[1] += rb[2] * dpx - rb[0] * dpz;
-                out.tp[2] += rb[0] * dpy - rb[1] * dpx;
-            }
+            out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz;   // only wall links reach here
         }
     } else {
         // ------------- FP32 arithmetic on stored deviations ---------------
@@ -336,6 +345,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
             if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
         }
         const float rho = 1.0f + dr;
+        if (GENERAL) out.rho = (double)rho;
         const float inv = 1.0f / rho;
         const float u = (jx + 0.5f * L.Ff[0]) * inv, v = (jy + 0.5f * L.Ff[1]) * inv, wz = (jz + 0.5f * L.Ff[2]) * inv;
         if (store_rho) a.rho[n] = 1.0 + (double)dr;
@@ -379,11 +389,12 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                     if (do_mass) out.mass += (double)S::rt(dpost);
                     continue;
                 }
-                double ub[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
-                if (GENERAL && tt == T_PARTICLE) {
-                    offset_from_squirmer(L, sq, x + 0.5 * CX(i), y + 0.5 * CY(i), z + 0.5 * CZ(i), rb);
-                    surface_velocity(sq, rb, ub, true);
+                if (GENERAL && tt == T_PARTICLE) {   // finished by zone_particle_links
+                    link_stash[i * BOUNDARY_BLOCK + threadIdx.x] = dpost;
+                    out.pmask |= 1u << i;
+                    continue;
                 }
+                const double ub[3] = {0, 0, 0};   // wall: u_b = 0
                 const double cub = CX(i) * ub[0] + CY(i) * ub[1] + CZ(i) * ub[2];
                 const double dl = 6.0 * WD(i) * (double)rho * cub;   // fpost - fb
                 const float dfb = (float)((double)dpost - dl);
@@ -394,13 +405,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                 const double dpx = sm * CX(i) - dl * ub[0];
                 const double dpy = sm * CY(i) - dl * ub[1];
                 const double dpz = sm * CZ(i) - dl * ub[2];
-                if (tt == T_WALL) { out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz; }
-                else {
-                    out.fp[0] += dpx; out.fp[1] += dpy; out.fp[2] += dpz;
-                    out.tp[0] += rb[1] * dpz - rb[2] * dpy;
-                    out.tp[1] += rb[2] * dpx - rb[0] * dpz;
-                    out.tp[2] += rb[0] * dpy - rb[1] * dpx;
-                }
+                out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz;   // only wall links reach here
             }
         }
     }
@@ -448,15 +453,71 @@ __global__ void __launch_bounds__(256, S::shifted ? 4 : 2) k_bulk(const Lattice 
 //  the next remap reads it) and write one row of link_part per near-particle
 //  node; wall force and mass go to block partials.
 // ---------------------------------------------------------------------------
-// The body of one zone thread (cell k of the zone); returns the sums for the
-// block reduction.
+// The particle links left by update_node<GENERAL> (lbm.cpp:189-215 with u_b
+// = U + W x r_b + slip, r_b at the link midpoint), finished by the whole warp
+// (every lane calls it): in round k each lane takes its k-th link in
+// ascending direction order, so the warp runs as many rounds as its busiest
+// lane has links instead of one pass per direction that any lane needs. The
+// arithmetic and the order of the per-node sums are those of the direction
+// loop in update_node.
+template <class S, int PAR>
+__device__ __forceinline__ void zone_particle_links(const Lattice& L, const StreamArgs& a, const SqState* sq,
+                                                    unsigned n, int x, int y, int z, bool do_mass,
+                                                    const LinkStash<S>* stash, NodeSums& out) {
+    using T = typename S::T;
+    T* __restrict__ f = static_cast<T*>(a.f);
+    unsigned m = out.pmask;
+    const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+    for (int k = 0; k < rounds; ++k) {
+        if (!m) continue;
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const int cx = c_cx[i], cy = c_cy[i], cz = c_cz[i];
+        const double w = c_w[i];
+        T* local = f + (size_t)opp_rt(i) * L.N + n;
+        T* remote = f + (size_t)i * L.N + nbr_rt(L, x, y, z, cx, cy, cz);
+        double rb[3], ub[3];
+        offset_from_squirmer(L, sq, x + 0.5 * cx, y + 0.5 * cy, z + 0.5 * cz, rb);
+        surface_velocity(sq, rb, ub, true);
+        const double cub = cx * ub[0] + cy * ub[1] + cz * ub[2];
+        double sm, dl;
+        if constexpr (!S::shifted) {
+            const double fpost = stash[i * BOUNDARY_BLOCK + threadIdx.x];
+            const double fb = fpost - 6.0 * w * out.rho * cub;
+            S::st(PAR == 0 ? remote : local, fb);
+            if (do_mass) out.mass += fb;
+            sm = fpost + fb;
+            dl = fpost - fb;
+        } else {
+            const float dpost = stash[i * BOUNDARY_BLOCK + threadIdx.x];
+            dl = 6.0 * w * out.rho * cub;   // fpost - fb
+            const float dfb = (float)((double)dpost - dl);
+            S::st(PAR == 0 ? remote : local, dfb);
+            if (do_mass) out.mass += (double)S::rt(dfb);
+            const double fpost = w + (double)dpost;
+            sm = 2.0 * fpost - dl;            // fpost + fb
+        }
+        const double dpx = sm * cx - dl * ub[0];
+        const double dpy = sm * cy - dl * ub[1];
+        const double dpz = sm * cz - dl * ub[2];
+        out.fp[0] += dpx; out.fp[1] += dpy; out.fp[2] += dpz;
+        out.tp[0] += rb[1] * dpz - rb[2] * dpy;
+        out.tp[1] += rb[2] * dpx - rb[0] * dpz;
+        out.tp[2] += rb[0] * dpy - rb[1] * dpx;
+    }
+}
+
+// Cell k of the zone, one per thread (every thread of the block calls it);
+// returns the sums for the block reduction. sq is the block's copy of the
+// squirmer state, stash the block's particle-link values.
 template <class S, int PAR, bool SQ, bool MACRO>
-__device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a, int k, NodeSums& sums) {
+__device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a, int k, NodeSums& sums,
+                                          const SqState* sq, LinkStash<S>* stash) {
     bool active = false;
     unsigned n = 0;
     int x = 0, y = 0, z = 0;
     if (SQ && k < a.zone_cells) {
-        const ZoneBox* zb = &a.sq->zone[a.zslot];
+        const ZoneBox* zb = &sq->zone[a.zslot];
         const int bx = k % a.zw[0], by = (k / a.zw[0]) % a.zw[1], bz = k / (a.zw[0] * a.zw[1]);
         x = zb->lo[0] + bx; if (x >= L.nx) x -= L.nx;
         y = zb->lo[1] + by; z = zb->lo[2] + bz;
@@ -467,10 +528,14 @@ __device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a,
             active = (a.flag[n] & TYPE_MASK) == T_FLUID;
         }
     }
+    uint8_t fl = 0;
     if (active) {
-        const uint8_t fl = a.flag[n];
-        update_node<S, PAR, true, MACRO>(L, a, n, x, y, z, fl, 0, SQ || MACRO, sums);
-        if (SQ && (fl & NEAR_PARTICLE)) {
+        fl = a.flag[n];
+        update_node<S, PAR, true, MACRO>(L, a, n, x, y, z, fl, 0, SQ || MACRO, sums, GlobalSrc(), stash);
+    }
+    if (SQ) {
+        zone_particle_links<S, PAR>(L, a, sq, n, x, y, z, a.do_mass != 0, stash, sums);
+        if (active && (fl & NEAR_PARTICLE)) {
             double* lp = a.link_part + (size_t)a.linkslot[n] * LINK_PART;
             lp[0] = sums.fp[0]; lp[1] = sums.fp[1]; lp[2] = sums.fp[2];
             lp[3] = sums.tp[0]; lp[4] = sums.tp[1]; lp[5] = sums.tp[2];
@@ -478,12 +543,23 @@ __device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a,
     }
 }
 
+// The squirmer state, one word per thread, into a block's shared copy.
+__device__ __forceinline__ void copy_sq_state(SqState* dst, const SqState* src) {
+    constexpr int NS = (int)(sizeof(SqState) / 4);
+    static_assert(sizeof(SqState) % 4 == 0 && NS <= BOUNDARY_BLOCK, "one word per thread");
+    if ((int)threadIdx.x < NS) reinterpret_cast<uint32_t*>(dst)[threadIdx.x] = reinterpret_cast<const uint32_t*>(src)[threadIdx.x];
+}
+
 template <class S, int PAR, bool SQ, bool MACRO>
 __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
     pdl_wait();
     pdl_launch_dependents();
+    __shared__ __align__(16) SqState zsq;
+    __shared__ LinkStash<S> stash[Q * BOUNDARY_BLOCK];
+    if (SQ) copy_sq_state(&zsq, a.sq);
+    __syncthreads();
     NodeSums sums;
-    zone_cell<S, PAR, SQ, MACRO>(L, a, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums);
+    zone_cell<S, PAR, SQ, MACRO>(L, a, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums, &zsq, stash);
     if (MACRO || a.do_mass)
         block_reduce4<BOUNDARY_BLOCK>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass,
                                       a.block_part_b + (size_t)blockIdx.x * BLOCK_PART);
