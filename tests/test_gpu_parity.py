@@ -42,6 +42,11 @@ CASES = {
     # duct walls and a squirmer near a z wall
     "boxwalls": dict(nx=30, ny=24, nz=24, tau=0.75, walls_y=1, walls_z=1, squirmer=1, radius=5.0, b1=0.012,
                      beta=1.0, angle=-10, planar=0, z0=8.0, y0=13.0),
+    # periodic box, a fast swimmer starting at x = 1 and heading in -x: its remap
+    # box wraps across the lattice edge, the sphere crosses it, and the cached
+    # candidate shell is rebuilt several times
+    "wrapx": dict(nx=24, ny=20, nz=20, tau=0.8, walls_y=0, walls_z=0, squirmer=1, radius=4.0, b1=0.03,
+                  beta=1.0, planar=0, ex=-0.9, ey=0.3, ez=0.2, x0=1.0),
 }
 
 
@@ -102,7 +107,7 @@ def test_single_step_bitwise_fp64(case, port, Solver):
             assert np.allclose(sg["Th"], so["Th"], rtol=1e-10, atol=1e-12)
 
 
-@pytest.mark.parametrize("case", ["slit", "bulk3d", "boxwalls"])
+@pytest.mark.parametrize("case", ["slit", "bulk3d", "boxwalls", "wrapx"])
 def test_advance_squirmer_remap_fp64(case, port, Solver):
     """Rigid-body update and cover/uncover remap (lbm.cpp:257-320), forced to
     move the sphere by 0.45 cells so that dozens of nodes change type."""
@@ -151,7 +156,8 @@ def test_correct_mass_fp64(case, port, Solver):
     assert abs(m - 1.0) < 1e-13
 
 
-@pytest.mark.parametrize("case,steps", [("duct", 1500), ("slit", 600), ("bulk3d", 400), ("boxwalls", 400)])
+@pytest.mark.parametrize("case,steps", [("duct", 1500), ("slit", 600), ("bulk3d", 400), ("boxwalls", 400),
+                                        ("wrapx", 600)])
 def test_run_matches_oracle_fp64(case, steps, port, Solver):
     """The fused device loop (CUDA graphs, deferred mass correction, device
     trajectory ring) against the oracle's time loop."""
