@@ -245,6 +245,61 @@ __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __r
 // GENERAL: the particle links are not computed here. Their post-collision
 // values go to link_stash[i * BOUNDARY_BLOCK + threadIdx.x], their directions
 // to out.pmask, and zone_particle_links finishes them with the whole warp.
+// FP64 collide and push of a node with only fluid neighbours, in the
+// reference's arithmetic (lbm.cpp:162-172, every operation in its order, no
+// contraction), one opposite pair (i, i+1) at a time. The terms of i+1 are
+// those of i with c -> -c: cu, c.F, feq-, f-, S- change sign exactly and feq+,
+// f+, S+ are equal, so they are formed once; fpost_{i+1} adds the negated odd
+// terms in the reference's order. The results are the reference's bits
+// (where a term is +-0 its sign may differ, which leaves a nonzero sum as it
+// is). FORCE = false drops the Guo terms: for F = 0 they are +-0.
+template <class S, int PAR, bool FORCE>
+__device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
+                                                 const Nbr& nb, const double* fv, double r, double u, double v,
+                                                 double wz, double usq, double uF, bool do_mass, NodeSums& out) {
+    const double Fx = L.F[0], Fy = L.F[1], Fz = L.F[2];
+    {   // rest population
+        const double cu = CX(0) * u + CY(0) * v + CZ(0) * wz;
+        const double cF = CX(0) * Fx + CY(0) * Fy + CZ(0) * Fz;
+        const double feqP = WD(0) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
+        const double feqM = WD(0) * r * 3.0 * cu;
+        const double fP = 0.5 * (fv[0] + fv[0]), fM = 0.5 * (fv[0] - fv[0]);
+        const double SP = WD(0) * (9.0 * cu * cF - 3.0 * uF), SM = WD(0) * 3.0 * cF;
+        const double fpost = FORCE ? fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM
+                                   : fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM);
+        S::st(f + n, fpost);
+        if (do_mass) out.mass += fpost;
+    }
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+        const int io = i + 1;
+        const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+        const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
+        const double feqM = WD(i) * r * 3.0 * cu;
+        const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
+        const double A = L.omP * (fP - feqP), B = L.omM * (fM - feqM);
+        double fi, fo;
+        if (FORCE) {
+            const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
+            const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
+            const double C = L.gP * SP, D = L.gM * SM;
+            fi = fv[i] - A - B + C + D;
+            fo = fv[io] - A + B + C - D;
+        } else {
+            fi = fv[i] - A - B;
+            fo = fv[io] - A + B;
+        }
+        if (PAR == 0) {
+            S::st(f + (size_t)io * N + n, fi);
+            S::st(f + (size_t)i * N + n, fo);
+        } else {
+            S::st(f + (size_t)i * N + nb.of(n, i), fi);
+            S::st(f + (size_t)io * N + nb.of(n, io), fo);
+        }
+        if (do_mass) { out.mass += fi; out.mass += fo; }
+    }
+}
+
 template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
                                             uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
@@ -287,6 +342,13 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
         if (GENERAL) out.rho = r;
         const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
+        if (!boundary) {   // every neighbour fluid: the pair form, same bits
+            if (L.force_free)
+                plain_pairs_fp64<S, PAR, false>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+            else
+                plain_pairs_fp64<S, PAR, true>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             // TRT + Guo forcing (lbm.cpp:162-172)
