@@ -487,8 +487,10 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
 //  squirmer update writes (except the correction value on the step after a
 //  correction step, when the launch waits for it).
 // ---------------------------------------------------------------------------
-template <class S, int PAR, bool SQ, bool MACRO, bool WR>
-__global__ void __launch_bounds__(256, S::shifted ? 4 : 2) k_bulk(const Lattice L, const StreamArgs a) {
+//    DENSE (FP64 only) 3 CTAs/SM instead of 2 (80 registers, a few spills): for
+//          long bulks; a short one leaves room for the zone and squirmer chain
+template <class S, int PAR, bool SQ, bool MACRO, bool WR, bool DENSE = false>
+__global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk(const Lattice L, const StreamArgs a) {
     pdl_wait();
     pdl_launch_dependents();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;

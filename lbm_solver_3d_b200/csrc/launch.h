@@ -18,6 +18,7 @@ struct StreamGeom {
     dim3 grid, block;
     unsigned bgrid;
     unsigned nwallrows;  // rows next to a wall (0: none)
+    bool dense;          // FP64: the bulk at 3 CTAs/SM (a long bulk)
 };
 
 struct SqArgs;

@@ -13,6 +13,12 @@ namespace lbmgpu {
 
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if constexpr (!S::shifted) {
+        if (g.dense) {
+            k_bulk<S, PAR, SQ, MACRO, false, true><<<g.grid, g.block, 0, st>>>(L, a);
+            return;
+        }
+    }
     k_bulk<S, PAR, SQ, MACRO, false><<<g.grid, g.block, 0, st>>>(L, a);
 }
 // Launch with programmatic stream serialisation: the kernel may be scheduled

@@ -628,6 +628,9 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     // squirmer; when the bulk moves less than ~200 MB (about 40 us) that chain
     // is the step, and they go after the bulk on stream a instead.
     h->wallrows_on_a = h->has_sq && (double)Q * 2.0 * h->esize * (double)N <= 200e6;
+    // FP64: a long bulk runs denser (3 CTAs/SM); a short one keeps 2, which
+    // leaves room on the SMs for the zone and squirmer chain beside it
+    h->geom.dense = (double)Q * 2.0 * h->esize * (double)N > 200e6;
     const int box = h->has_sq ? 2 * (int)std::ceil(p->radius) + 8 : 1;
     const long long boxvol = (long long)box * box * box;
     h->link_cap = (int)std::max<long long>(boxvol, (long long)hi.links.size() + 1);
