@@ -232,7 +232,11 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_c
 // g, g + G, g + 2G, ... (G = all warps). The member records are copied only
 // when the member changes, and the next chunk's descriptor is loaded while
 // the current chunk is updated, so a warp's start-up latency is paid once.
-template <class S, int PAR, bool MACRO>
+// FLAT (steps without sums): the chunks are 32-node pieces of runs of rows,
+// x0 in the low 16 bits of ChunkRef::x0 and the length above; a piece starts
+// at (x0, y) and continues into the next rows of the same z-plane, and no
+// partials are written.
+template <class S, int PAR, bool MACRO, bool FLAT = false>
 __global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_chunkp(
     const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args, const ChunkRef* __restrict__ chunks,
     int nchunks, double* __restrict__ chunk_part, BatchStep st) {
@@ -270,13 +274,22 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_c
         const Lattice& L = sL[w];
         const StreamArgs& a = sA[w];
         NodeSums sums;
-        const int x = cr.x0 + lane;
-        if (x < L.nx) {
-            const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)cr.y + (unsigned)L.ny * (unsigned)cr.z);
-            const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, cr.y, cr.z);
-            if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, cr.y, cr.z, 0, 0, MACRO, sums);
+        int x, y = cr.y;
+        bool on;
+        if (FLAT) {
+            x = (cr.x0 & 0xffff) + lane;
+            on = lane < (cr.x0 >> 16);
+            while (x >= L.nx) { x -= L.nx; ++y; }
+        } else {
+            x = cr.x0 + lane;
+            on = x < L.nx;
         }
-        if (st.do_mass || MACRO) {
+        if (on) {
+            const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)cr.z);
+            const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, y, cr.z);
+            if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, y, cr.z, 0, 0, MACRO, sums);
+        }
+        if (!FLAT && (st.do_mass || MACRO)) {
             chunk_reduce(sums);
             if (lane == 0) {
                 double* o = chunk_part + (size_t)c * BLOCK_PART;

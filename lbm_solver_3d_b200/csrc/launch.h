@@ -38,6 +38,7 @@ struct BatchArgs {
     const int* bounds;                 // staged kernel: row range of each CTA (grid + 1 entries)
     const ChunkRef* chunks; int nchunks;   // chunk kernel: 32-node pieces of the rows away from walls
     const RowChunks* rowchunks;        // chunk kernel: each row's chunks
+    const ChunkRef* flat; int nflat;   // persistent chunk kernel, steps without sums: 32-node pieces of row runs
     double* chunk_part;                // chunk kernel: partial sums per chunk
     int cap;                           // staged kernel: elements per staged direction-row
     int fcap;                          // staged kernel: bytes per staged flag row

@@ -160,6 +160,10 @@ static void chunk_one(bool sums, const BatchArgs& b, BatchStep st, cudaStream_t 
 template <class S, int PAR, bool MACRO>
 static void chunkp_one(int grid, bool sums, const BatchArgs& b, BatchStep st, cudaStream_t s) {
     if (b.nchunks == 0) return;
+    if (!sums && b.nflat > 0) {   // no partial sums this step: the run pieces
+        k_bulk_chunkp<S, PAR, MACRO, true><<<grid, 32 * CHUNK_WARPS, 0, s>>>(b.lat, b.args, b.flat, b.nflat, nullptr, st);
+        return;
+    }
     k_bulk_chunkp<S, PAR, MACRO><<<grid, 32 * CHUNK_WARPS, 0, s>>>(b.lat, b.args, b.chunks, b.nchunks, b.chunk_part, st);
     if (sums) k_fold_chunks<<<(b.nrows + 255) / 256, 256, 0, s>>>(b.rowchunks, b.nrows, b.chunk_part, b.row_part);
 }

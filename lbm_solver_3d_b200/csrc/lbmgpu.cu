@@ -1254,6 +1254,7 @@ struct lbmgpu_batch {
     int tile = LBMGPU_TILE_CHUNKP, bps = 4;   // bps: resident CTAs per SM, set at creation
     int* d_bounds = nullptr;       // staged kernel: row range of each CTA
     ChunkRef* d_chunks = nullptr;  // chunk kernel
+    ChunkRef* d_flat = nullptr;    // persistent chunk kernel, steps without sums
     RowChunks* d_rowchunks = nullptr;
     double* chunk_part = nullptr;
     int bounds_cap = 0, bounds_grid = 0;
@@ -1290,7 +1291,7 @@ void batch_free(lbmgpu_batch* b) {
     b->m.clear();
     void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts,
                     b->row_part, b->zone_part, b->d_status, b->d_bounds, b->d_chunks, b->d_rowchunks,
-                    b->chunk_part};
+                    b->chunk_part, b->d_flat};
     for (void* q : ptrs) if (q) cudaFree(q);
     for (cudaEvent_t e : {b->ev_b[0], b->ev_b[1], b->ev_z, b->ev_s, b->ev_fork, b->ev_join})
         if (e) cudaEventDestroy(e);
@@ -1546,6 +1547,29 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
         rowchunks[r] = RowChunks{(int)chunks.size(), (nx + 31) / 32, rows[r].part, 0};
         for (int x0 = 0; x0 < nx; x0 += 32) chunks.push_back(ChunkRef{rows[r].m, rows[r].y, rows[r].z, x0});
     }
+    // Runs of consecutive rows away from walls in one z-plane of one member are
+    // contiguous in memory; on steps without sums the persistent chunk kernel
+    // walks them in full 32-node pieces ([x0, x0 + len) from row y, continuing
+    // into the next rows), so no lane idles at a row's end.
+    std::vector<ChunkRef> flat;
+    for (size_t r = 0; r < rows.size();) {
+        size_t e = r + 1;
+        while (e < rows.size() && rows[e].m == rows[r].m && rows[e].z == rows[r].z &&
+               rows[e].y == rows[e - 1].y + 1)
+            ++e;
+        const int nx = ps[rows[r].m].nx;
+        const long long total = (long long)(e - r) * nx;
+        for (long long o = 0; o < total; o += 32) {
+            const int len = (int)std::min<long long>(32, total - o);
+            const int y = rows[r].y + (int)(o / nx), x0 = (int)(o % nx);
+            flat.push_back(ChunkRef{rows[r].m, y, rows[r].z, x0 | (len << 16)});
+        }
+        r = e;
+    }
+    CB(cudaMalloc(&b->d_flat, std::max<size_t>(1, flat.size()) * sizeof(ChunkRef)));
+    if (!flat.empty())
+        CB(cudaMemcpyAsync(b->d_flat, flat.data(), flat.size() * sizeof(ChunkRef), cudaMemcpyHostToDevice, b->sa));
+    b->ba.flat = b->d_flat; b->ba.nflat = (int)flat.size();
     CB(cudaMalloc(&b->d_chunks, std::max<size_t>(1, chunks.size()) * sizeof(ChunkRef)));
     CB(cudaMalloc(&b->d_rowchunks, std::max<size_t>(1, rowchunks.size()) * sizeof(RowChunks)));
     CB(cudaMalloc(&b->chunk_part, std::max<size_t>(1, chunks.size()) * BLOCK_PART * sizeof(double)));
