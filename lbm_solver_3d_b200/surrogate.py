@@ -12,7 +12,7 @@ Uses:
     answered by the surrogate only while its whole trajectory stays inside the
     training hull and the networks of the ensemble agree; every other point is
     run with the full LBM (an ``Ensemble``), which is the fallback and the
-    judge of the surrogate's error;
+    measure of the surrogate's error;
   * ``Surrogate.warm_start`` the velocities that start an LBM run of the
     near-wall phase at the surrogate's state instead of at rest.
 

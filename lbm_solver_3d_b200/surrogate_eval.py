@@ -1,5 +1,5 @@
-"""Train the swimmer surrogate on LBM ensemble trajectories and judge it with
-the LBM on held-out members (different seed: new beta, angle, height, sizes).
+"""Train the swimmer surrogate on LBM ensemble trajectories and evaluate it
+against the LBM on held-out members (different seed: new beta, angle, height, sizes).
 
     python -m lbm_solver_3d_b200.surrogate_eval --data DIR [--out report.json]
 

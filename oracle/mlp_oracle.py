@@ -10,7 +10,7 @@ W4[3][64] b4[3], W[out][in] (the layout of include/lbmgpu.h).
 The surrogate has no counterpart in the reference (it is one of the forms
 built beside the plain method), so there is no reference code to pin this
 restatement to; it is pinned to central finite differences of its own loss
-(tests/test_mlp.py) and is the judge of the GPU gradients.
+(tests/test_mlp.py) and is what the GPU gradients are checked against.
 """
 from __future__ import annotations
 

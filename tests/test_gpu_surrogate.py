@@ -1,6 +1,6 @@
 """The surrogate end to end on a small sweep: LBM ensemble -> training data ->
-networks trained by the library's kernels -> held-out drift velocities judged
-by the LBM.
+networks trained by the library's kernels -> held-out drift velocities checked
+against the LBM.
 
 Small configuration (about a minute on one B200): 48 training and 8 held-out
 slit channels of reduced size (Nx 48-80, Ny, Nz 32-48, a 3-5), 6000 steps,
