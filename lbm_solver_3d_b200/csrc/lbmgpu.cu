@@ -1717,7 +1717,7 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     BTRY(b, cudaEventCreate(&e1));
     const int tiles[8] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_CHUNKP, LBMGPU_TILE_ROWCTA, 32, 64, 128,
                           LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4};
-    const int bpss[7] = {1, 2, 3, 4, 5, 6, 8};
+    const int bpss[8] = {1, 2, 3, 4, 5, 6, 7, 8};
     double best = 1e30;
     int btx = b->tile, bbps = b->bps;
     const BatchStep bst{(int)((b->t + 1) % ZONE_SLOTS), 0, 0};
