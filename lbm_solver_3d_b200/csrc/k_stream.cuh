@@ -300,6 +300,43 @@ __device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T
     }
 }
 
+// The post-collision populations of all 19 directions in the pair form of
+// plain_pairs_fp64 (the reference's bits), for the boundary path.
+template <bool FORCE>
+__device__ __forceinline__ void collide_pairs_fp64(const Lattice& L, const double* fv, double r, double u, double v,
+                                                   double wz, double usq, double uF, double* post) {
+    const double Fx = L.F[0], Fy = L.F[1], Fz = L.F[2];
+    {
+        const double cu = CX(0) * u + CY(0) * v + CZ(0) * wz;
+        const double cF = CX(0) * Fx + CY(0) * Fy + CZ(0) * Fz;
+        const double feqP = WD(0) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
+        const double feqM = WD(0) * r * 3.0 * cu;
+        const double fP = 0.5 * (fv[0] + fv[0]), fM = 0.5 * (fv[0] - fv[0]);
+        const double SP = WD(0) * (9.0 * cu * cF - 3.0 * uF), SM = WD(0) * 3.0 * cF;
+        post[0] = FORCE ? fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM
+                        : fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM);
+    }
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+        const int io = i + 1;
+        const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+        const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
+        const double feqM = WD(i) * r * 3.0 * cu;
+        const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
+        const double A = L.omP * (fP - feqP), B = L.omM * (fM - feqM);
+        if (FORCE) {
+            const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
+            const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
+            const double C = L.gP * SP, D = L.gM * SM;
+            post[i] = fv[i] - A - B + C + D;
+            post[io] = fv[io] - A + B + C - D;
+        } else {
+            post[i] = fv[i] - A - B;
+            post[io] = fv[io] - A + B;
+        }
+    }
+}
+
 template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
                                             uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
@@ -349,17 +386,14 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                 plain_pairs_fp64<S, PAR, true>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
             return;
         }
+        // TRT + Guo forcing (lbm.cpp:162-172), in the pair form
+        double post[Q];
+        if (L.force_free) collide_pairs_fp64<false>(L, fv, r, u, v, wz, usq, uF, post);
+        else collide_pairs_fp64<true>(L, fv, r, u, v, wz, usq, uF, post);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
-            // TRT + Guo forcing (lbm.cpp:162-172)
             const int io = OPP(i);
-            const double cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-            const double cF = CX(i) * Fx + CY(i) * Fy + CZ(i) * Fz;
-            const double feqP = WD(i) * r * (1.0 + 4.5 * cu * cu - 1.5 * usq);
-            const double feqM = WD(i) * r * 3.0 * cu;
-            const double fP = 0.5 * (fv[i] + fv[io]), fM = 0.5 * (fv[i] - fv[io]);
-            const double SP = WD(i) * (9.0 * cu * cF - 3.0 * uF), SM = WD(i) * 3.0 * cF;
-            const double fpost = fv[i] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM;
+            const double fpost = post[i];
             const unsigned nbi = nb.of(n, i);
             T* local = f + (size_t)io * N + n;
             T* remote = f + (size_t)i * N + nbi;
