@@ -56,6 +56,7 @@ def evaluate(s: Surrogate, table, rows, transient: int, tol: float = 0.05):
         v_bulk = U0 * np.array([np.cos(th0[i]), np.sin(th0[i])])
         nv = np.linalg.norm(v_lbm)
         out.append(dict(member=i, beta=p.beta, a=p.R, H_over_a=(p.NY - 2) / p.R, h0_over_a=(y0[i] - 0.5) / p.R,
+                        nx=p.NX, nz=p.NZ,
                         theta0=float(th0[i]), v_lbm=v_lbm.tolist(), v_surrogate=v_sur.tolist(),
                         err_surrogate=float(np.linalg.norm(v_sur - v_lbm) / nv),
                         err_bulk_speed=float(np.linalg.norm(v_bulk - v_lbm) / nv),
@@ -100,6 +101,17 @@ def main():
         by_tol[str(tol)] = {"trusted_members": int(tr.sum()),
                             "max_err_trusted": float(e_s[tr].max()) if tr.any() else None}
     dgen = np.load(d / "surrogate_heldout.npz")
+    # does the error follow what the four inputs leave out, the periodic box
+    # length and width (the swimmer's images)? Spearman rank correlations
+    def spearman(u, v):
+        ru, rv = np.argsort(np.argsort(u)), np.argsort(np.argsort(v))
+        return float(np.corrcoef(ru, rv)[0, 1])
+    a_nx = np.array([m["a"] / m["nx"] for m in per_member])
+    a_nz = np.array([m["a"] / m["nz"] for m in per_member])
+    h_a = np.array([m["h0_over_a"] for m in per_member])
+    bet = np.array([m["beta"] for m in per_member])
+    corr = {"a/Nx": spearman(e_s, a_nx), "a/Nz": spearman(e_s, a_nz), "h0/a": spearman(e_s, h_a),
+            "|beta|": spearman(e_s, np.abs(bet))}
     report = {
         "samples_train": int((~vmask).sum()) * 2, "samples_val": int(vmask.sum()),
         "samples_heldout": int(len(hx)), "gemm": "fp32" if args.fp32 else "bf16", "nets": args.nets,
@@ -118,6 +130,7 @@ def main():
         "trust_tolerance_sweep": by_tol,
         "drift_rel_err_trusted_only": {"max": float(e_s[trusted].max()) if trusted.any() else None,
                                        "median": float(np.median(e_s[trusted])) if trusted.any() else None},
+        "err_rank_correlation": corr,
         "time_surrogate_s": t_sur,
         "time_lbm_s": float(dgen["seconds"]),
         "per_member": per_member,
