@@ -107,7 +107,11 @@ class Surrogate:
     @classmethod
     def fit(cls, x, y, x_val=None, y_val=None, n_nets: int = 3, bf16: bool = True, epochs: int = 40,
             batch: int = 512, lr: float = 2e-3, lr_min: float = 5e-5, seed: int = 0, device: int = 0,
-            augment: bool = True):
+            augment: bool = True, beta_emphasis: float = 0.0):
+        """beta_emphasis w > 0 draws each epoch's samples with replacement, with
+        probability proportional to 1 + w (|beta| / max |beta|)^2: the strong
+        pushers and pullers, whose near-wall dynamics carry most of the
+        held-out error, are seen more often."""
         import time
         if augment:
             xa, ya = mirror(x, y)
@@ -115,6 +119,11 @@ class Surrogate:
         xm, xs = x.mean(0), x.std(0) + 1e-12
         ym, ys = y.mean(0), y.std(0) + 1e-12
         xn, yn = ((x - xm) / xs).astype(np.float32), ((y - ym) / ys).astype(np.float32)
+        prob = None
+        if beta_emphasis > 0:
+            b = np.abs(x[:, 2]) / max(np.abs(x[:, 2]).max(), 1e-12)
+            prob = 1.0 + beta_emphasis * b * b
+            prob /= prob.sum()
         nets, logs = [], []
         t0 = time.time()
         for k in range(n_nets):
@@ -124,7 +133,8 @@ class Surrogate:
             tl, vl = [], []
             for ep in range(epochs):
                 cur = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * ep / max(1, epochs - 1)))
-                tl.append(net.train_epoch(rng.permutation(len(xn)), batch=batch, lr=cur))
+                order = rng.permutation(len(xn)) if prob is None else rng.choice(len(xn), size=len(xn), p=prob)
+                tl.append(net.train_epoch(order, batch=batch, lr=cur))
                 if x_val is not None:
                     pv = net.forward((x_val - xm) / xs) * ys + ym
                     vl.append(float(np.mean(((pv - y_val) / ys) ** 2)))

@@ -76,6 +76,8 @@ def main():
     ap.add_argument("--window", type=int, default=0,
                     help="train on velocities from central differences over +-window rows (0: instantaneous)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--beta-emphasis", type=float, default=0.0,
+                    help="draw training samples with probability 1 + w (|beta|/max)^2 (0: plain permutation)")
     args = ap.parse_args()
     d = Path(args.data)
     table, rows, x, y, mem = dataset_from_npz(d / "surrogate_train.npz", args.transient, args.window)
@@ -85,7 +87,7 @@ def main():
     vmask = np.isin(mem, val_members)
     t0 = time.time()
     s = Surrogate.fit(x[~vmask], y[~vmask], x[vmask], y[vmask], n_nets=args.nets, bf16=not args.fp32,
-                      epochs=args.epochs, seed=args.seed)
+                      epochs=args.epochs, seed=args.seed, beta_emphasis=args.beta_emphasis)
     t_fit = time.time() - t0
     htable, hrows, hx, hy, hmem = dataset_from_npz(d / "surrogate_heldout.npz", args.transient)
     pred, spread = s.predict(hx)
@@ -115,7 +117,7 @@ def main():
     report = {
         "samples_train": int((~vmask).sum()) * 2, "samples_val": int(vmask.sum()),
         "samples_heldout": int(len(hx)), "gemm": "fp32" if args.fp32 else "bf16", "nets": args.nets,
-        "window": args.window,
+        "window": args.window, "beta_emphasis": args.beta_emphasis,
         "epochs": args.epochs, "fit_seconds": t_fit,
         "val_loss_final": [lg.val_loss[-1] for lg in s.logs],
         "heldout_instantaneous_velocity_rel_err": {"median": float(np.median(inst)), "mean": float(inst.mean()),
