@@ -301,7 +301,9 @@ __device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T
 }
 
 // The post-collision populations of all 19 directions in the pair form of
-// plain_pairs_fp64 (the reference's bits), for the boundary path.
+// plain_pairs_fp64 (the reference's bits), for the boundary path. The bulk
+// keeps its own copy of these lines, which stores each pair as soon as it is
+// formed: written through this helper it spills more at 3 CTAs/SM.
 template <bool FORCE>
 __device__ __forceinline__ void collide_pairs_fp64(const Lattice& L, const double* fv, double r, double u, double v,
                                                    double wz, double usq, double uF, double* post) {
