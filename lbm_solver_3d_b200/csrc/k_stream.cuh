@@ -547,6 +547,28 @@ __global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk(
     }
 }
 
+// k_bulk_flat<S, PAR, SQ, DENSE>: the nodes of k_bulk on a step without sums
+// (no mass correction, no macroscopic output), for lattices whose nx is not a
+// multiple of 32. The rows away from walls of one z-plane are one contiguous
+// range of nodes; 256 threads take 256 consecutive nodes of it, so no lane
+// idles at a row's end. Grid (ceil(range / 256), planes away from z walls).
+template <class S, int PAR, bool SQ, bool DENSE = false>
+__global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk_flat(const Lattice L, const StreamArgs a) {
+    pdl_wait();
+    pdl_launch_dependents();
+    const int ylo = L.walls_y ? 2 : 0, rows = L.walls_y ? L.ny - 4 : L.ny;
+    const int z = (L.walls_z ? 2 : 0) + (int)blockIdx.y;
+    const int o = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (o >= rows * L.nx) return;
+    const int dy = o / L.nx;
+    const int x = o - dy * L.nx, y = ylo + dy;
+    const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+    bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0;
+    if (SQ && active) active = !in_zone(L, a.sq->zone[a.zslot], x, y, z);
+    NodeSums sums;
+    if (active) update_node<S, PAR, false, false>(L, a, n, x, y, z, 0, 0, false, sums);
+}
+
 // ---------------------------------------------------------------------------
 //  k_zone<S, PAR, SQ, MACRO>: thread k updates the fluid node at cell k of the
 //  zone (row-major, x fastest). Zone nodes store rho every step (the refill of

@@ -13,6 +13,11 @@ namespace lbmgpu {
 
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if (!MACRO && !a.do_mass && g.flat.x) {   // no sums this step: whole rows of nodes per block
+        if (!S::shifted && g.dense) k_bulk_flat<S, PAR, SQ, true><<<g.flat, 256, 0, st>>>(L, a);
+        else k_bulk_flat<S, PAR, SQ><<<g.flat, 256, 0, st>>>(L, a);
+        return;
+    }
     if constexpr (!S::shifted) {
         if (g.dense) {
             k_bulk<S, PAR, SQ, MACRO, false, true><<<g.grid, g.block, 0, st>>>(L, a);

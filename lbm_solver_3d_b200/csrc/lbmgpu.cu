@@ -631,6 +631,15 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     // FP64: a long bulk runs denser (3 CTAs/SM); a short one keeps 2, which
     // leaves room on the SMs for the zone and squirmer chain beside it
     h->geom.dense = (double)Q * 2.0 * h->esize * (double)N > 200e6;
+    // nx not a multiple of 32: on steps without sums the bulk runs over each
+    // plane's rows away from walls as one range of nodes (no idle lanes)
+    {
+        const int rows = p->walls_y ? p->ny - 4 : p->ny, planes = p->walls_z ? p->nz - 4 : p->nz;
+        const long long range = (long long)rows * p->nx;
+        h->geom.flat = dim3(0, 0, 0);
+        if (p->nx % 32 != 0 && rows > 0 && planes > 0)
+            h->geom.flat = dim3((unsigned)((range + 255) / 256), (unsigned)planes, 1);
+    }
     const int box = h->has_sq ? 2 * (int)std::ceil(p->radius) + 8 : 1;
     const long long boxvol = (long long)box * box * box;
     h->link_cap = (int)std::max<long long>(boxvol, (long long)hi.links.size() + 1);
