@@ -135,6 +135,31 @@ int lbmgpu_squirmer_state(lbmgpu_handle* h, lbmgpu_squirmer* s);
  * uncovered nodes overridden by the refill. Any pointer may be NULL. */
 int lbmgpu_fields(lbmgpu_handle* h, uint8_t* flag, double* rho, double* u3);
 
+/* Asynchronous snapshot of the same fields, for writers that run beside the
+ * time loop (replaces the reference's writeVTK reading the solver's host
+ * arrays between two steps, io.cpp:44-67 called from main.cpp:67).
+ * lbmgpu_snapshot_begin queues, after the work already issued on the
+ * handle's stream, a device-side copy of the node types, rho and u of the
+ * last step into a snapshot buffer of the handle (allocated on the first
+ * call, 33 bytes per node) and returns at once: the time loop may continue.
+ * lbmgpu_snapshot_read waits for that copy only (not for steps queued after
+ * it) and copies the snapshot into the host buffers, laid out as for
+ * lbmgpu_fields, on a stream of its own, so the copy overlaps the steps
+ * running meanwhile. It may be called from another host thread while the
+ * owning thread keeps advancing the lattice (it touches only the snapshot);
+ * its failures are reported by lbmgpu_snapshot_last_error. One snapshot at a
+ * time: _begin returns LBMGPU_ERR_INVALID while the previous one is unread.
+ * Host buffers from lbmgpu_host_alloc make the copies faster. */
+int lbmgpu_snapshot_begin(lbmgpu_handle* h);
+int lbmgpu_snapshot_read(lbmgpu_handle* h, uint8_t* flag, double* rho, double* u3);
+const char* lbmgpu_snapshot_last_error(const lbmgpu_handle* h);
+
+/* Page-locked host memory (cudaHostAlloc) for buffers that receive fields or
+ * snapshots: the device copies into it directly instead of through a staging
+ * buffer. NULL on failure; free with lbmgpu_host_free. */
+void* lbmgpu_host_alloc(size_t bytes);
+int lbmgpu_host_free(void* p);
+
 /* Diagnostics replacing countFluid/meanDensity/maxSpeed/sumUx and wallForce. */
 int lbmgpu_diag(lbmgpu_handle* h, lbmgpu_diagnostics* d);
 
@@ -157,12 +182,21 @@ int lbmgpu_set_populations(lbmgpu_handle* h, const double* f);
  * buffer: the stored populations (storage form and AA parity as they are),
  * flags, rho/u of the last step, the squirmer state with its zones, pending
  * mass correction and counters, the boundary-link list and the trajectory
- * ring. Loading it into a lattice created with the same parameters continues
- * the run bit for bit. _size gives the bytes _save needs; _load checks the
- * lattice sizes, storage form and squirmer presence and rejects a mismatch. */
+ * ring, behind a header that records the deck the state belongs to (sizes,
+ * storage form, walls, tau, lambda, body force, cadences, squirmer model).
+ * Loading it into a lattice created with the same parameters continues the
+ * run bit for bit. _size gives the bytes _save needs. _load validates the
+ * whole buffer on the host before anything reaches the device: the header
+ * against the lattice's parameters, every link node index (inside the
+ * lattice, ascending, a fluid node next to the sphere), the zone boxes, the
+ * counters and the node types against the wall layers. A mismatch or a
+ * corrupt buffer returns LBMGPU_ERR_INVALID and leaves the lattice as it was.
+ * _check runs the same validation against parameters alone (no device, no
+ * handle), e.g. to reject a restart file before creating the lattice. */
 int lbmgpu_checkpoint_size(lbmgpu_handle* h, size_t* bytes);
 int lbmgpu_checkpoint_save(lbmgpu_handle* h, void* buf, size_t len);
 int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len);
+int lbmgpu_checkpoint_check(const lbmgpu_params* p, const void* buf, size_t len, char* msg, size_t msg_len);
 
 /* Overwrite the rigid-body state X, e, U, W (seeded parity cases, restart).
  * The lattice mapping is not changed. */
@@ -264,6 +298,8 @@ const char* lbmgpu_mlp_last_error(const lbmgpu_mlp* m);
  * 256^3 x 2); larger sizes return LBMGPU_ERR_INVALID with a message.
  * Set-up: the first call on each device looks up the scratch's address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The lookup is repeated when the device's context has been recreated
+ * (cudaDeviceReset), whose module load may place the array elsewhere.
  * Concurrency: the scratch is one per device and shared by all callers, so
  * calls that overlap on a device (from several host threads, or on several
  * streams) race and corrupt each other's results: serialise them.

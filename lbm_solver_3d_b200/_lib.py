@@ -14,6 +14,8 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "lib" / "liblbmgpu.so"
 
 LBMGPU_OK = 0
+LBMGPU_ERR_INVALID, LBMGPU_ERR_CUDA, LBMGPU_ERR_NAN, LBMGPU_ERR_DEVICE = -1, -2, -3, -4
+LBMGPU_ERR_NOMEM, LBMGPU_ERR_WATCHDOG = -5, -6
 STATUS = {0: "OK", -1: "INVALID", -2: "CUDA", -3: "NAN", -4: "DEVICE", -5: "NOMEM", -6: "WATCHDOG"}
 
 
@@ -91,9 +93,16 @@ SIGNATURES = {
     "lbmgpu_mlp_forward": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float)]),
     "lbmgpu_mlp_forward_ex": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float), _I]),
     "lbmgpu_mlp_last_error": (ctypes.c_char_p, [_P]),
+    "lbmgpu_snapshot_begin": (_I, [_P]),
+    "lbmgpu_snapshot_read": (_I, [_P, _U8P, _DP, _DP]),
+    "lbmgpu_snapshot_last_error": (ctypes.c_char_p, [_P]),
+    "lbmgpu_host_alloc": (_P, [ctypes.c_size_t]),
+    "lbmgpu_host_free": (_I, [_P]),
     "lbmgpu_checkpoint_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "lbmgpu_checkpoint_save": (_I, [_P, _P, ctypes.c_size_t]),
     "lbmgpu_checkpoint_load": (_I, [_P, _P, ctypes.c_size_t]),
+    "lbmgpu_checkpoint_check": (_I, [ctypes.POINTER(LbmgpuParams), _P, ctypes.c_size_t, ctypes.c_char_p,
+                                     ctypes.c_size_t]),
     "lbmgpu_batch_create": (_I, [ctypes.POINTER(LbmgpuParams), _I, ctypes.POINTER(_P)]),
     "lbmgpu_batch_destroy": (_I, [_P]),
     "lbmgpu_batch_run": (_I, [_P, _I]),

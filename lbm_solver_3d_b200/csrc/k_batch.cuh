@@ -340,8 +340,11 @@ static __global__ void k_fold_chunks(const RowChunks* __restrict__ rc, int nrows
 //  SM sit in shared memory rather than in registers. Row partial sums are
 //  formed as in k_bulk_batch (bit-identical to a lattice run alone).
 //  Every wait is bounded: on a timeout ST_WATCHDOG is set in the member's
-//  status word and the CTA stops. There is no CTA-wide barrier after the
-//  start, so a stopped warp cannot leave the others waiting unboundedly.
+//  status word and the CTA stops. The only CTA-wide barrier after the start
+//  is the last one, which every warp reaches once its own loop has ended (all
+//  its waits are bounded). Behind it, after an abort, one thread waits
+//  (bounded) for the last copy the producer issued into each stage, so no bulk
+//  copy is still landing in this CTA's shared memory when it exits.
 // ---------------------------------------------------------------------------
 constexpr int STAGED_UPDATE_WARPS = 4;
 constexpr int STAGED_THREADS = 32 * (1 + STAGED_UPDATE_WARPS);
@@ -440,6 +443,7 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
     __shared__ double red[NST][BATCH_CHUNKS][4];   // chunk sums of the row in stage q
     __shared__ int cnt[NST];                        // update warps done with the row in stage q
     __shared__ volatile int s_abort;
+    __shared__ int s_issued;                        // stages armed by the producer
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int r0 = bounds[blockIdx.x], r1 = bounds[blockIdx.x + 1];
     const bool sums_on = st.do_mass || MACRO;
@@ -452,6 +456,7 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
+        s_issued = 0;
     }
     __syncthreads();
 
@@ -519,11 +524,10 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
                 bulk_g2s(buf + ((size_t)q * Q + lane) * cap, reinterpret_cast<const void*>(start), len, &full[q]);
             else if (lane == Q)
                 bulk_g2s(fbuf + (size_t)q * fcap, reinterpret_cast<const void*>(start), len, &full[q]);
+            if (lane == 0) s_issued = k + 1;
             __syncwarp();
         }
-        return;
-    }
-
+    } else {
     // ---------------- update warps ----------------
     const int ut = tid - 32;   // 0 .. 32 * STAGED_UPDATE_WARPS - 1
     for (int k = 0; r0 + k < r1; ++k) {
@@ -578,6 +582,18 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
                 }
             }
             mbar_arrive(&empty[q]);   // the stage (and red[q]) may be refilled
+        }
+    }
+    }
+    // After an abort, stage q may still receive the copies of its last arming
+    // (the update warps stopped waiting for them): wait for that phase to
+    // complete before the CTA's shared memory is released.
+    __syncthreads();
+    if (tid == 0 && s_abort) {
+        const int issued = s_issued;
+        for (int q = 0; q < NST && q < issued; ++q) {
+            const int arms = (issued - q + NST - 1) / NST;   // times stage q was armed
+            mbar_wait(&full[q], (uint32_t)((arms - 1) & 1));
         }
     }
 }

@@ -413,11 +413,12 @@ __global__ void __launch_bounds__(TC_M) k_mlp_fwd_tc(const float* __restrict__ p
     const uint32_t my_lanes = tmem + ((uint32_t)(warp * 32) << 16);
 
     bool ok = true;
-    uint32_t phase = 0;
+    uint32_t phase = 0, last = 0;   // last: the phase of the most recent commit
     const void* Ws[3] = {&S.W1[0][0][0], &S.W2[0][0][0], &S.W3[0][0][0]};
     const float* bs[3] = {S.b1, S.b2, S.b3};
     for (int l = 0; l < 3 && ok; ++l) {
         if (tid == 0) tc_layer(tmem, &S.A[0][0][0], Ws[l], l == 0 ? PI_ : NH, NH, &S.mbar);
+        last = phase;
         ok = __all_sync(0xffffffffu, tc_wait(&S.mbar, phase));   // warp-uniform: tcgen05.ld is .sync.aligned
         phase ^= 1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -440,6 +441,7 @@ __global__ void __launch_bounds__(TC_M) k_mlp_fwd_tc(const float* __restrict__ p
     }
     if (ok) {
         if (tid == 0) tc_layer(tmem, &S.A[0][0][0], &S.W4[0][0][0], NH, PO, &S.mbar);
+        last = phase;
         ok = __all_sync(0xffffffffu, tc_wait(&S.mbar, phase));
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (ok) {
@@ -450,7 +452,18 @@ __global__ void __launch_bounds__(TC_M) k_mlp_fwd_tc(const float* __restrict__ p
                 for (int o = 0; o < NO; ++o) Yout[(size_t)row * NO + o] = y[o] + S.b4[o];
         }
     }
-    if (!ok && tid == 0) atomicExch(err, 1);
+    ok = __syncthreads_and(ok);   // the same verdict in every warp
+    if (!ok) {
+        // A wait gave up while the last layer's MMAs may still be writing
+        // tensor memory: wait (bounded) for their commit before the columns
+        // are freed.
+        if (tid == 0) {
+            atomicExch(err, 1);
+            tc_wait(&S.mbar, last);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_COLS));

@@ -199,38 +199,74 @@ struct GlobalSrc {
     }
 };
 
+// Moments of a node in the shifted forms, from its 19 stored numbers d (storage
+// units: the deviation times S::SC): dr = sum of d, rho, and the Guo
+// half-force velocity (lbm.cpp:143-152).
+template <class S>
+__device__ __forceinline__ void shifted_moments(const Lattice& L, const float* d, float& dr, float& rho, float& u,
+                                                float& v, float& wz) {
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+    dr = 0.f;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        dr += d[i];
+        if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
+        if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
+        if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
+    }
+    rho = 1.0f + dr * S::INV;
+    const float inv = 1.0f / rho;
+    u = (jx * S::INV + 0.5f * L.Ff[0]) * inv;
+    v = (jy * S::INV + 0.5f * L.Ff[1]) * inv;
+    wz = (jz * S::INV + 0.5f * L.Ff[2]) * inv;
+}
+
+// TRT + Guo post-collision values in storage units (lbm.cpp:162-172, deviation
+// form): the rest population, and one opposite pair (i, i+1) with f+, feq+ and
+// S+ shared and the odd parts of opposite signs. srho = S::SC * rho, k15 =
+// 1.5 |u|^2, uF = u . F. FORCE = false drops the Guo source terms, which
+// vanish for F = 0.
+template <class S, bool FORCE>
+__device__ __forceinline__ float rest_post(const Lattice& L, float d0, float dr, float srho, float k15, float uF) {
+    const float eP = WF(0) * (dr - srho * k15);
+    return FORCE ? d0 - L.omPf * (d0 - eP) - S::SC * L.gPf * WF(0) * 3.0f * uF : d0 - L.omPf * (d0 - eP);
+}
+template <class S, bool FORCE>
+__device__ __forceinline__ void pair_post(const Lattice& L, int i, float di, float dio, float u, float v, float wz,
+                                          float dr, float srho, float k15, float uF, float& oi, float& oo) {
+    const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+    const float w = WF(i);
+    const float eP = w * (dr + srho * (4.5f * cu * cu - k15));  // feq+ - w, storage units
+    const float eM = 3.0f * w * srho * cu;                       // feq-
+    const float fP = 0.5f * (di + dio), fM = 0.5f * (di - dio);
+    float A, B;
+    if (FORCE) {
+        A = S::SC * L.gPf * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - L.omPf * (fP - eP);
+        B = S::SC * L.cm[i] - L.omMf * (fM - eM);
+    } else {
+        A = -L.omPf * (fP - eP);
+        B = -L.omMf * (fM - eM);
+    }
+    oi = di + A + B;
+    oo = dio + A - B;
+}
+
 // Collide and push of a node with only fluid neighbours, FP32 arithmetic on
-// stored deviations: the rest population, then one opposite pair (i, i+1) at a
-// time (f+, feq+ and S+ shared by the pair, the odd parts with opposite
-// signs). FORCE = false drops the Guo source terms, which vanish for F = 0.
+// stored numbers: the rest population, then one opposite pair at a time.
 template <class S, int PAR, bool FORCE>
 __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
-                                            const Nbr& nb, const float* d, float dr, float rho, float u, float v,
+                                            const Nbr& nb, const float* d, float dr, float srho, float u, float v,
                                             float wz, float uF, float k15, bool do_mass, NodeSums& out) {
-    const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
     {   // rest population: c = 0
-        const float eP = WF(0) * (dr - rho * k15);
-        const float o0 = FORCE ? d[0] - omP * (d[0] - eP) - gP * WF(0) * 3.0f * uF : d[0] - omP * (d[0] - eP);
+        const float o0 = rest_post<S, FORCE>(L, d[0], dr, srho, k15, uF);
         S::st(f + n, o0);
-        if (do_mass) out.mass += (double)S::rt(o0);
+        if (do_mass) out.mass += (double)S::rt(o0) * S::INV;
     }
 #pragma unroll
     for (int i = 1; i < Q; i += 2) {
         const int io = i + 1;
-        const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-        const float w = WF(i);
-        const float eP = w * (dr + rho * (4.5f * cu * cu - k15));  // feq+ - w
-        const float eM = 3.0f * w * rho * cu;                       // feq-
-        const float fP = 0.5f * (d[i] + d[io]), fM = 0.5f * (d[i] - d[io]);
-        float A, B;
-        if (FORCE) {
-            A = gP * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - omP * (fP - eP);
-            B = L.cm[i] - omM * (fM - eM);
-        } else {
-            A = -omP * (fP - eP);
-            B = -omM * (fM - eM);
-        }
-        const float oi = d[i] + A + B, oo = d[io] + A - B;
+        float oi, oo;
+        pair_post<S, FORCE>(L, i, d[i], d[io], u, v, wz, dr, srho, k15, uF, oi, oo);
         if (PAR == 0) {
             S::st(f + (size_t)io * N + n, oi);
             S::st(f + (size_t)i * N + n, oo);
@@ -238,7 +274,7 @@ __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __r
             S::st(f + (size_t)i * N + nb.of(n, i), oi);
             S::st(f + (size_t)io * N + nb.of(n, io), oo);
         }
-        if (do_mass) out.mass += (double)S::rt(oi) + (double)S::rt(oo);
+        if (do_mass) out.mass += (double)S::rt(oi) * S::INV + (double)S::rt(oo) * S::INV;
     }
 }
 
@@ -426,53 +462,34 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
             out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz;   // only wall links reach here
         }
     } else {
-        // ------------- FP32 arithmetic on stored deviations ---------------
+        // ------- FP32 arithmetic on stored deviations (storage units) --------
         float d[Q];
         src.template load<S, PAR>(f, N, n, nb, d);
         if (a.apply_corr) {
             const double corr = sq->corr_d;
 #pragma unroll
-            for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * corr);
+            for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * corr * S::SC);
         }
-        float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            dr += d[i];
-            if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
-            if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
-            if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
-        }
-        const float rho = 1.0f + dr;
+        float dr, rho, u, v, wz;
+        shifted_moments<S>(L, d, dr, rho, u, v, wz);
         if (GENERAL) out.rho = (double)rho;
-        const float inv = 1.0f / rho;
-        const float u = (jx + 0.5f * L.Ff[0]) * inv, v = (jy + 0.5f * L.Ff[1]) * inv, wz = (jz + 0.5f * L.Ff[2]) * inv;
-        if (store_rho) a.rho[n] = 1.0 + (double)dr;
+        if (store_rho) a.rho[n] = 1.0 + (double)dr * S::INV;
         if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
         const float usq = u * u + v * v + wz * wz;
         const float uF = u * L.Ff[0] + v * L.Ff[1] + wz * L.Ff[2];
-        const float omP = L.omPf, omM = L.omMf, gP = L.gPf;
         const float k15 = 1.5f * usq;
+        const float srho = S::SC * rho;
         if (!boundary) {
             if (L.force_free)   // uniform: the Guo source terms are exactly zero
-                plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, rho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
             else
-                plain_pairs<S, PAR, true>(L, f, N, n, nb, d, dr, rho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, true>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
         } else {
             float post[Q];
-            post[0] = d[0] - omP * (d[0] - WF(0) * (dr - rho * k15)) - gP * WF(0) * 3.0f * uF;
+            post[0] = rest_post<S, true>(L, d[0], dr, srho, k15, uF);
 #pragma unroll
-            for (int i = 1; i < Q; i += 2) {
-                const int io = i + 1;
-                const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-                const float w = WF(i);
-                const float eP = w * (dr + rho * (4.5f * cu * cu - k15));
-                const float eM = 3.0f * w * rho * cu;
-                const float fP = 0.5f * (d[i] + d[io]), fM = 0.5f * (d[i] - d[io]);
-                const float A = gP * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - omP * (fP - eP);
-                const float B = L.cm[i] - omM * (fM - eM);
-                post[i] = d[i] + A + B;
-                post[io] = d[io] + A - B;
-            }
+            for (int i = 1; i < Q; i += 2)
+                pair_post<S, true>(L, i, d[i], d[i + 1], u, v, wz, dr, srho, k15, uF, post[i], post[i + 1]);
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
                 const float dpost = post[i];
@@ -484,7 +501,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                                              : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
                 if (tt == T_FLUID) {
                     S::st(PAR == 0 ? local : remote, dpost);
-                    if (do_mass) out.mass += (double)S::rt(dpost);
+                    if (do_mass) out.mass += (double)S::rt(dpost) * S::INV;
                     continue;
                 }
                 if (GENERAL && tt == T_PARTICLE) {   // finished by zone_particle_links
@@ -494,11 +511,11 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                 }
                 const double ub[3] = {0, 0, 0};   // wall: u_b = 0
                 const double cub = CX(i) * ub[0] + CY(i) * ub[1] + CZ(i) * ub[2];
-                const double dl = 6.0 * WD(i) * (double)rho * cub;   // fpost - fb
-                const float dfb = (float)((double)dpost - dl);
+                const double dl = 6.0 * WD(i) * (double)rho * cub;   // fpost - fb (deviation units)
+                const float dfb = (float)((double)dpost - dl * S::SC);
                 S::st(PAR == 0 ? remote : local, dfb);
-                if (do_mass) out.mass += (double)S::rt(dfb);
-                const double fpost = WD(i) + (double)dpost;
+                if (do_mass) out.mass += (double)S::rt(dfb) * S::INV;
+                const double fpost = WD(i) + (double)dpost * S::INV;
                 const double sm = 2.0 * fpost - dl;                   // fpost + fb
                 const double dpx = sm * CX(i) - dl * ub[0];
                 const double dpy = sm * CY(i) - dl * ub[1];
@@ -570,6 +587,151 @@ __global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk_
 }
 
 // ---------------------------------------------------------------------------
+//  k_bulk_pair<S, PAR, SQ, FORCE>: the nodes of k_bulk on a step without sums
+//  (no mass correction, no macroscopic output) in the shifted forms, two
+//  x-adjacent nodes (x0, x0 + 1) per thread, x0 even. Every direction moves
+//  both nodes' values with one 2-element load and one 2-element store (8 B in
+//  FP32, 4 B in FP16), so a warp touches 64 consecutive nodes of a direction
+//  row per instruction. Requires nx a multiple of 64 (whole warps of pairs,
+//  aligned vectors); blockDim.x divides nx / 2 (a multiple of 32, at most
+//  PAIR_BLOCK), grid (nx / 2 / blockDim.x, ny, nz), rows next to a wall
+//  skipped (their own launch).
+//
+//  Even steps read and write the node's own slots A[i][n], A[opp(i)][n]: both
+//  aligned pairs. Odd steps read A[opp(i)][n - c_i] and write A[i][n + c_i],
+//  one cell off in x for the directions with c_x != 0. Such a direction is
+//  moved as aligned pairs all the same and the x shift made across lanes:
+//    load, source x - 1: node x0 takes the previous lane's upper element,
+//      x0 + 1 its own lower one; source x + 1: node x0 its own upper element,
+//      x0 + 1 the next lane's lower one;
+//    store, target x + 1: the aligned pair (x0, x0 + 1) holds the previous
+//      lane's x0 - 1 value and this lane's x0 value; target x - 1: this lane's
+//      x0 + 1 value and the next lane's x0 + 2 value.
+//  A lane whose neighbour in that direction is in another warp, or across the
+//  periodic x boundary, loads or stores that element alone. A node that the
+//  bulk does not update (the zone, a node next to the sphere) is neither read
+//  into nor written by a vector: the pair is split into single elements.
+//  The per-node arithmetic is that of update_node's force-free / forced
+//  branches (shifted_moments, rest_post, pair_post), so results are those of
+//  k_bulk bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int PAIR_BLOCK = 128;
+
+template <class S, int PAR, bool SQ, bool FORCE>
+__global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, const StreamArgs a) {
+    using T = typename S::T;
+    pdl_wait();
+    pdl_launch_dependents();
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (wall_row(L, y, z)) return;   // block-uniform: the wall-row launch owns this row
+    T* __restrict__ f = static_cast<T*>(a.f);
+    const unsigned N = L.N;
+    const int lane = threadIdx.x & 31;
+    const int x0 = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const unsigned row = (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+    const unsigned n0 = row + (unsigned)x0;
+    bool act0 = (a.flag[n0] & (uint8_t)~NEAR_WALL) == 0;
+    bool act1 = (a.flag[n0 + 1] & (uint8_t)~NEAR_WALL) == 0;
+    if (SQ) {
+        const ZoneBox zb = a.sq->zone[a.zslot];
+        act0 = act0 && !in_zone(L, zb, x0, y, z);
+        act1 = act1 && !in_zone(L, zb, x0 + 1, y, z);
+    }
+    // lanes whose pair neighbour in x sits in the same warp (no periodic wrap)
+    const bool has_prev = lane > 0 && x0 > 0;
+    const bool has_next = lane < 31 && x0 + 2 < L.nx;
+    const bool prev_act1 = __shfl_up_sync(0xffffffffu, act1, 1) && has_prev;
+    const bool next_act0 = __shfl_down_sync(0xffffffffu, act0, 1) && has_next;
+    const int xm = x0 == 0 ? L.nx - 1 : x0 - 1;        // x0 - 1, wrapped
+    const int xp = x0 + 2 == L.nx ? 0 : x0 + 2;        // x0 + 2, wrapped
+    // row offsets of the y/z neighbours (periodic wrap as in Nbr)
+    const int yp = (y == L.ny - 1) ? (1 - L.ny) * L.nx : L.nx;
+    const int ym = (y == 0) ? (L.ny - 1) * L.nx : -L.nx;
+    const int zp = (z == L.nz - 1) ? (1 - L.nz) * (int)L.nxy : (int)L.nxy;
+    const int zm = (z == 0) ? (L.nz - 1) * (int)L.nxy : -(int)L.nxy;
+    auto ryz = [&](int i) {   // row offset of n + c_i in y and z
+        return (CY(i) > 0 ? yp : (CY(i) < 0 ? ym : 0)) + (CZ(i) > 0 ? zp : (CZ(i) < 0 ? zm : 0));
+    };
+
+    // ---- loads: logical f_i of both nodes ----
+    float d0[Q], d1[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (PAR == 0) {
+            const float2 q = S::ld2(f + (size_t)i * N + n0);
+            d0[i] = q.x; d1[i] = q.y;
+        } else {
+            const int o = OPP(i);                              // read A[o][n + c_o]
+            const T* rowp = f + (size_t)o * N + (size_t)((int)row + ryz(o));
+            const float2 q = S::ld2(rowp + x0);
+            if (CX(o) == 0) {
+                d0[i] = q.x; d1[i] = q.y;
+            } else if (CX(o) < 0) {                            // source x - 1
+                const float up = __shfl_up_sync(0xffffffffu, q.y, 1);
+                d0[i] = has_prev ? up : S::ld(rowp + xm);
+                d1[i] = q.x;
+            } else {                                           // source x + 1
+                const float dn = __shfl_down_sync(0xffffffffu, q.x, 1);
+                d0[i] = q.y;
+                d1[i] = has_next ? dn : S::ld(rowp + xp);
+            }
+        }
+    }
+    if (a.apply_corr) {
+        const double corr = a.sq->corr_d;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const float c = (float)(WD(i) * corr * S::SC);
+            d0[i] += c; d1[i] += c;
+        }
+    }
+    float dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
+    shifted_moments<S>(L, d0, dr0, rho0, u0, v0, w0);
+    shifted_moments<S>(L, d1, dr1, rho1, u1, v1, w1);
+    const float k0 = 1.5f * (u0 * u0 + v0 * v0 + w0 * w0), k1 = 1.5f * (u1 * u1 + v1 * v1 + w1 * w1);
+    const float uF0 = u0 * L.Ff[0] + v0 * L.Ff[1] + w0 * L.Ff[2];
+    const float uF1 = u1 * L.Ff[0] + v1 * L.Ff[1] + w1 * L.Ff[2];
+    const float sr0 = S::SC * rho0, sr1 = S::SC * rho1;
+
+    // ---- stores: post-collision value of direction i to its slot ----
+    // (a, b) = values of nodes x0, x0 + 1 for direction i
+    auto put = [&](int i, float a0, float a1) {
+        if (PAR == 0) {                                        // A[opp(i)][n]
+            T* p = f + (size_t)OPP(i) * N + n0;
+            if (act0 && act1) S::st2(p, a0, a1);
+            else { if (act0) S::st(p, a0); if (act1) S::st(p + 1, a1); }
+            return;
+        }
+        T* rowp = f + (size_t)i * N + (size_t)((int)row + ryz(i));   // A[i][n + c_i]
+        if (CX(i) == 0) {
+            if (act0 && act1) S::st2(rowp + x0, a0, a1);
+            else { if (act0) S::st(rowp + x0, a0); if (act1) S::st(rowp + x0 + 1, a1); }
+        } else if (CX(i) > 0) {                                // targets x0 + 1, x0 + 2
+            const float pv = __shfl_up_sync(0xffffffffu, a1, 1);
+            if (prev_act1 && act0) S::st2(rowp + x0, pv, a0);
+            else { if (prev_act1) S::st(rowp + x0, pv); if (act0) S::st(rowp + x0 + 1, a0); }
+            if (!has_next && act1) S::st(rowp + xp, a1);
+        } else {                                               // targets x0 - 1, x0
+            const float nv = __shfl_down_sync(0xffffffffu, a0, 1);
+            if (act1 && next_act0) S::st2(rowp + x0, a1, nv);
+            else { if (act1) S::st(rowp + x0, a1); if (next_act0) S::st(rowp + x0 + 1, nv); }
+            if (!has_prev && act0) S::st(rowp + xm, a0);
+        }
+    };
+    put(0, rest_post<S, FORCE>(L, d0[0], dr0, sr0, k0, uF0), rest_post<S, FORCE>(L, d1[0], dr1, sr1, k1, uF1));
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+        float a0i, a0o, a1i, a1o;
+        pair_post<S, FORCE>(L, i, d0[i], d0[i + 1], u0, v0, w0, dr0, sr0, k0, uF0, a0i, a0o);
+        pair_post<S, FORCE>(L, i, d1[i], d1[i + 1], u1, v1, w1, dr1, sr1, k1, uF1, a1i, a1o);
+        // direction i's post value goes where the next state reads logical
+        // f_i: even step -> A[opp(i)][n]; odd step -> A[i][n + c_i]
+        put(i, a0i, a1i);
+        put(i + 1, a0o, a1o);
+    }
+}
+
+// ---------------------------------------------------------------------------
 //  k_zone<S, PAR, SQ, MACRO>: thread k updates the fluid node at cell k of the
 //  zone (row-major, x fastest). Zone nodes store rho every step (the refill of
 //  the next remap reads it) and write one row of link_part per near-particle
@@ -611,12 +773,12 @@ __device__ __forceinline__ void zone_particle_links(const Lattice& L, const Stre
             sm = fpost + fb;
             dl = fpost - fb;
         } else {
-            const float dpost = stash[i * BOUNDARY_BLOCK + threadIdx.x];
-            dl = 6.0 * w * out.rho * cub;   // fpost - fb
-            const float dfb = (float)((double)dpost - dl);
+            const float dpost = stash[i * BOUNDARY_BLOCK + threadIdx.x];   // storage units
+            dl = 6.0 * w * out.rho * cub;   // fpost - fb (deviation units)
+            const float dfb = (float)((double)dpost - dl * S::SC);
             S::st(PAR == 0 ? remote : local, dfb);
-            if (do_mass) out.mass += (double)S::rt(dfb);
-            const double fpost = w + (double)dpost;
+            if (do_mass) out.mass += (double)S::rt(dfb) * S::INV;
+            const double fpost = w + (double)dpost * S::INV;
             sm = 2.0 * fpost - dl;            // fpost + fb
         }
         const double dpx = sm * cx - dl * ub[0];

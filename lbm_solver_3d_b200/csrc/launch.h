@@ -20,6 +20,7 @@ struct StreamGeom {
     unsigned nwallrows;  // rows next to a wall (0: none)
     bool dense;          // FP64: the bulk at 3 CTAs/SM (a long bulk)
     dim3 flat;           // k_bulk_flat's grid for steps without sums (x = 0: not used)
+    dim3 pair, pair_block;   // k_bulk_pair's grid and block for steps without sums (x = 0: not used)
 };
 
 struct SqArgs;

@@ -51,27 +51,43 @@ constexpr int ST_WATCHDOG = 16;      // a bounded wait for staged data gave up
 // ---- storage forms ----------------------------------------------------------
 // FP64: f_i itself. FP32 / FP16: the deviation f_i - w_i rho0 (rho0 = 1), FP16
 // scaled by 2^12 so that typical deviations (1e-8 .. 0.05) stay normal.
+// The stream kernels work in storage units: ld/st/rt move the stored number
+// as it is (for FP16 the scaled deviation), and SC / INV convert between
+// storage units and deviations (1 for FP32, so its arithmetic is unchanged).
+// T2 is the 2-element vector of the stored type (two x-adjacent nodes).
 struct StoreF64 {
     using T = double;
+    using T2 = double2;
     static constexpr bool shifted = false;
+    static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static double ld(const T* p) { return *p; }
     __device__ static void st(T* p, double v) { *p = v; }
     __device__ static double rt(double v) { return v; }  // value as it will be stored
 };
 struct StoreF32 {
     using T = float;
+    using T2 = float2;
     static constexpr bool shifted = true;
+    static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static float ld(const T* p) { return *p; }
     __device__ static void st(T* p, float v) { *p = v; }
     __device__ static float rt(float v) { return v; }
+    __device__ static float2 ld2(const T* p) { return *reinterpret_cast<const float2*>(p); }
+    __device__ static void st2(T* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
 };
 constexpr float FP16_SCALE = 4096.0f, FP16_INV_SCALE = 1.0f / 4096.0f;
 struct StoreF16 {
     using T = __half;
+    using T2 = __half2;
     static constexpr bool shifted = true;
-    __device__ static float ld(const T* p) { return __half2float(*p) * FP16_INV_SCALE; }
-    __device__ static void st(T* p, float v) { *p = __float2half_rn(v * FP16_SCALE); }
-    __device__ static float rt(float v) { return __half2float(__float2half_rn(v * FP16_SCALE)) * FP16_INV_SCALE; }
+    static constexpr float SC = FP16_SCALE, INV = FP16_INV_SCALE;
+    __device__ static float ld(const T* p) { return __half2float(*p); }
+    __device__ static void st(T* p, float v) { *p = __float2half_rn(v); }
+    __device__ static float rt(float v) { return __half2float(__float2half_rn(v)); }
+    __device__ static float2 ld2(const T* p) { return __half22float2(*reinterpret_cast<const __half2*>(p)); }
+    __device__ static void st2(T* p, float a, float b) {
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+    }
 };
 
 // ---- lattice description (kernel argument, fixed per handle) ---------------

@@ -13,6 +13,13 @@ namespace lbmgpu {
 
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if constexpr (S::shifted && !MACRO) {
+        if (!a.do_mass && g.pair.x) {   // no sums this step: two x-adjacent nodes per thread
+            if (L.force_free) k_bulk_pair<S, PAR, SQ, false><<<g.pair, g.pair_block, 0, st>>>(L, a);
+            else k_bulk_pair<S, PAR, SQ, true><<<g.pair, g.pair_block, 0, st>>>(L, a);
+            return;
+        }
+    }
     if (!MACRO && !a.do_mass && g.flat.x) {   // no sums this step: whole rows of nodes per block
         if (!S::shifted && g.dense) k_bulk_flat<S, PAR, SQ, true><<<g.flat, 256, 0, st>>>(L, a);
         else k_bulk_flat<S, PAR, SQ><<<g.flat, 256, 0, st>>>(L, a);

@@ -25,7 +25,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -109,6 +111,16 @@ struct lbmgpu_handle {
     // ensemble member: populations and flags live in the ensemble's pools,
     // work is issued by the ensemble on its streams
     bool member = false;
+
+    // packed fields for the host (allocated on first use): rho (N doubles),
+    // u interleaved (3N doubles), node types (N bytes) -- one buffer for
+    // lbmgpu_fields, one for the asynchronous snapshot
+    unsigned char* packed = nullptr;
+    unsigned char* snap = nullptr;
+    cudaStream_t snap_stream = nullptr;   // the snapshot's copies to the host
+    cudaEvent_t snap_ready = nullptr;     // the snapshot's packing is done
+    std::atomic<bool> snap_pending{false};
+    std::string snap_err;
 };
 
 // ---------------------------------------------------------------------------
@@ -137,6 +149,20 @@ const Launchers* launchers_for(int prec) {
 }
 
 size_t esize_for(int prec) { return prec == LBMGPU_FP64 ? 8 : (prec == LBMGPU_FP32 ? 4 : 2); }
+
+// LBMGPU_PAIR_BULK=0 in the environment keeps the one-node bulk kernel on
+// every step (for comparing the two; results are the same bit for bit).
+bool pair_bulk_disabled() {
+    const char* e = std::getenv("LBMGPU_PAIR_BULK");
+    return e && e[0] == '0';
+}
+
+// Capacity of the boundary-link list of a lattice with these parameters (the
+// links lie inside the sphere's box, so the box volume bounds them).
+int link_capacity(const lbmgpu_params& p) {
+    const int box = p.squirmer ? 2 * (int)std::ceil(p.radius) + 8 : 1;
+    return (int)((long long)box * box * box);
+}
 
 // Settings of time step s (1-based).
 struct StepPlan {
@@ -247,6 +273,21 @@ __global__ void k_diag_final(const double* part, int nparts, double* out) {
     double a = 0, b = 0, d = 0, e = 0;
     for (int k = 0; k < nparts; ++k) { a += part[4 * k]; b += part[4 * k + 1]; d = fmax(d, part[4 * k + 2]); e += part[4 * k + 3]; }
     out[0] = a; out[1] = b; out[2] = d; out[3] = e;
+}
+
+// The fields the writers read, packed for one copy each to the host: rho,
+// u interleaved as (ux, uy, uz) per node, and the node type (low two flag bits).
+__global__ void k_pack_fields(unsigned N, const uint8_t* __restrict__ flag, const double* __restrict__ rho,
+                              const double* __restrict__ ux, const double* __restrict__ uy,
+                              const double* __restrict__ uz, double* __restrict__ prho, double* __restrict__ pu,
+                              uint8_t* __restrict__ pflag) {
+    for (unsigned n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+        prho[n] = rho[n];
+        pu[3 * (size_t)n] = ux[n];
+        pu[3 * (size_t)n + 1] = uy[n];
+        pu[3 * (size_t)n + 2] = uz[n];
+        pflag[n] = flag[n] & TYPE_MASK;
+    }
 }
 
 // ---- host-side restatement of the initial state ----------------------------
@@ -414,11 +455,12 @@ void free_all(lbmgpu_handle* h) {
     if (h->member) { h->f = nullptr; h->flag = nullptr; }
     void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wallrows, h->links, h->linkslot,
                     h->link_part, h->block_part, h->block_part_b, h->ordermap, h->chg_node, h->chg_key,
-                    h->cand, h->mark, h->traj, h->sq, h->scratch, h->small, h->shell, h->shell_hdr};
+                    h->cand, h->mark, h->traj, h->sq, h->scratch, h->small, h->shell, h->shell_hdr,
+                    h->packed, h->snap};
     for (void* q : ptrs) if (q) cudaFree(q);
-    for (cudaEvent_t e : {h->ev_b[0], h->ev_b[1], h->ev_z, h->ev_s, h->ev_fork, h->ev_join})
+    for (cudaEvent_t e : {h->ev_b[0], h->ev_b[1], h->ev_z, h->ev_s, h->ev_fork, h->ev_join, h->snap_ready})
         if (e) cudaEventDestroy(e);
-    for (cudaStream_t s : {h->own, h->zs, h->cap, h->cap2})
+    for (cudaStream_t s : {h->own, h->zs, h->cap, h->cap2, h->snap_stream})
         if (s) cudaStreamDestroy(s);
 }
 
@@ -499,6 +541,27 @@ int ensure_graph(lbmgpu_handle* h, int steps) {
     CUDA_TRY(h, cudaGraphInstantiate(&h->g.exec, h->g.graph, 0));
     h->g.steps = steps;
     return LBMGPU_OK;
+}
+
+// Packed fields (k_pack_fields): rho, u interleaved, node types.
+struct PackedView {
+    double* rho;
+    double* u;
+    uint8_t* flag;
+};
+PackedView packed_view(const lbmgpu_handle* h, unsigned char* base) {
+    const size_t N = h->L.N;
+    return PackedView{reinterpret_cast<double*>(base), reinterpret_cast<double*>(base) + N,
+                      reinterpret_cast<uint8_t*>(base + 4 * N * sizeof(double))};
+}
+cudaError_t ensure_packed(lbmgpu_handle* h, unsigned char** buf) {
+    if (*buf) return cudaSuccess;
+    return cudaMalloc(reinterpret_cast<void**>(buf), (size_t)h->L.N * (4 * sizeof(double) + 1));
+}
+void pack_fields(lbmgpu_handle* h, unsigned char* buf, cudaStream_t st) {
+    const PackedView v = packed_view(h, buf);
+    k_pack_fields<<<1184, 256, 0, st>>>(h->L.N, h->flag, h->rho, h->ux, h->uy, h->uz, v.rho, v.u, v.flag);
+    ++h->launches;
 }
 
 int check_status(lbmgpu_handle* h) {
@@ -639,11 +702,25 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
         h->geom.flat = dim3(0, 0, 0);
         if (p->nx % 32 != 0 && rows > 0 && planes > 0)
             h->geom.flat = dim3((unsigned)((range + 255) / 256), (unsigned)planes, 1);
+        // shifted forms, nx a multiple of 64: on steps without sums the bulk
+        // updates two x-adjacent nodes per thread (k_bulk_pair); the block is
+        // the largest multiple of 32 up to 128 threads that divides nx / 2
+        h->geom.pair = dim3(0, 0, 0);
+        if (p->precision != LBMGPU_FP64 && p->nx % 64 == 0 && !pair_bulk_disabled()) {
+            const int pairs = p->nx / 2;
+            int tb = 32;
+            for (int b = 128; b >= 32; b -= 32)
+                if (pairs % b == 0) { tb = b; break; }
+            h->geom.pair_block = dim3((unsigned)tb, 1, 1);
+            h->geom.pair = dim3((unsigned)(pairs / tb), (unsigned)p->ny, (unsigned)p->nz);
+        }
     }
-    const int box = h->has_sq ? 2 * (int)std::ceil(p->radius) + 8 : 1;
-    const long long boxvol = (long long)box * box * box;
-    h->link_cap = (int)std::max<long long>(boxvol, (long long)hi.links.size() + 1);
-    h->chg_cap = (int)boxvol;
+    h->link_cap = link_capacity(*p);
+    h->chg_cap = h->link_cap;
+    if ((long long)hi.links.size() >= h->link_cap) {
+        h->err = "boundary-link list of the initial state exceeds its capacity";
+        return bail(LBMGPU_ERR_DEVICE);
+    }
     {
         const int tx = p->nx >= 256 ? 256 : ((p->nx + 31) / 32) * 32;
         h->geom.block = dim3(tx, 1, 1);
@@ -881,19 +958,62 @@ int lbmgpu_fields(lbmgpu_handle* h, uint8_t* flag, double* rho, double* u3) {
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     const size_t N = h->L.N;
     cudaStream_t st = h->stream;
-    if (flag) CUDA_TRY(h, cudaMemcpyAsync(flag, h->flag, N, cudaMemcpyDeviceToHost, st));
-    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, h->rho, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-    std::vector<double> tmp;
-    if (u3) {
-        tmp.resize(3 * N);
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->ux, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.data() + N, h->uy, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.data() + 2 * N, h->uz, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-    }
+    CUDA_TRY(h, ensure_packed(h, &h->packed));
+    pack_fields(h, h->packed, st);
+    const PackedView v = packed_view(h, h->packed);
+    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, v.rho, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (u3) CUDA_TRY(h, cudaMemcpyAsync(u3, v.u, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (flag) CUDA_TRY(h, cudaMemcpyAsync(flag, v.flag, N, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(h, cudaStreamSynchronize(st));
-    if (flag) for (size_t n = 0; n < N; ++n) flag[n] &= TYPE_MASK;
-    if (u3)
-        for (size_t n = 0; n < N; ++n) { u3[3 * n] = tmp[n]; u3[3 * n + 1] = tmp[N + n]; u3[3 * n + 2] = tmp[2 * N + n]; }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_snapshot_begin(lbmgpu_handle* h) {
+    if (!h) return LBMGPU_ERR_INVALID;
+    if (h->snap_pending.load()) return fail(h, LBMGPU_ERR_INVALID, "the previous snapshot has not been read");
+    CUDA_TRY(h, cudaSetDevice(h->p.device));
+    CUDA_TRY(h, ensure_packed(h, &h->snap));
+    if (!h->snap_stream) {
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+    }
+    pack_fields(h, h->snap, h->stream);   // after everything issued on the handle's stream so far
+    CUDA_TRY(h, cudaEventRecord(h->snap_ready, h->stream));
+    CUDA_TRY(h, cudaGetLastError());
+    h->snap_pending.store(true);
+    return LBMGPU_OK;
+}
+
+int lbmgpu_snapshot_read(lbmgpu_handle* h, uint8_t* flag, double* rho, double* u3) {
+    if (!h) return LBMGPU_ERR_INVALID;
+    if (!h->snap_pending.load()) { h->snap_err = "no snapshot taken (lbmgpu_snapshot_begin)"; return LBMGPU_ERR_INVALID; }
+    const size_t N = h->L.N;
+    const PackedView v = packed_view(h, h->snap);
+    cudaStream_t st = h->snap_stream;
+    cudaError_t e = cudaSetDevice(h->p.device);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->snap_ready, 0);
+    if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, v.rho, N * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && u3) e = cudaMemcpyAsync(u3, v.u, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && flag) e = cudaMemcpyAsync(flag, v.flag, N, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    h->snap_pending.store(false);
+    if (e != cudaSuccess) {
+        h->snap_err = std::string("lbmgpu_snapshot_read: ") + cudaGetErrorString(e);
+        return LBMGPU_ERR_CUDA;
+    }
+    return LBMGPU_OK;
+}
+
+const char* lbmgpu_snapshot_last_error(const lbmgpu_handle* h) { return h ? h->snap_err.c_str() : ""; }
+
+void* lbmgpu_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0 || cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    return p;
+}
+
+int lbmgpu_host_free(void* p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) return LBMGPU_ERR_CUDA;
     return LBMGPU_OK;
 }
 
@@ -955,6 +1075,14 @@ int lbmgpu_traj_rows(lbmgpu_handle* h, double* rows, int max_rows, int* nrows, l
 // trajectory counters), the boundary-link list and the trajectory ring. A
 // lattice created with the same parameters and loaded from it continues bit
 // for bit as the saved one would have.
+//
+// The header records every parameter the stored state depends on (sizes,
+// storage form, walls, the TRT and forcing constants, the squirmer model and
+// the cadences). Loading checks them against the lattice's own parameters and
+// checks every index in the payload on the host (link nodes, zone boxes,
+// counters, node types against the wall layers) before anything is copied to
+// the device, so a checkpoint of another deck or a corrupt file is rejected
+// with LBMGPU_ERR_INVALID instead of reaching a kernel.
 namespace {
 struct CkptHeader {
     char magic[8];
@@ -963,15 +1091,112 @@ struct CkptHeader {
     int64_t t_main, traj_read;
     int32_t pending_corr, n_links;
     uint64_t f_bytes, sq_bytes;
+    // the deck of the stored state (version 2)
+    int32_t walls_y, walls_z, planar, mass_correction_every, traj_every, reserved;
+    double tau, lambda, fx, fy, fz, radius, b1, beta, rho_p, eps, hc, hmin;
 };
 constexpr char CKPT_MAGIC[8] = {'L', 'B', 'M', 'G', 'P', 'U', 'C', 'K'};
+constexpr uint32_t CKPT_VERSION = 2;
 
-size_t ckpt_bytes(const lbmgpu_handle* h, int n_links) {
-    const size_t N = h->L.N;
-    size_t b = sizeof(CkptHeader) + (size_t)Q * N * h->esize + N + 4 * N * sizeof(double) + sizeof(SqState);
-    if (h->has_sq) b += (size_t)n_links * sizeof(int) + (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double);
+size_t ckpt_payload(const lbmgpu_params& p, int n_links) {
+    const size_t N = (size_t)p.nx * p.ny * p.nz;
+    size_t b = sizeof(CkptHeader) + (size_t)Q * N * esize_for(p.precision) + N + 4 * N * sizeof(double) + sizeof(SqState);
+    if (p.squirmer) b += (size_t)n_links * sizeof(int) + (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double);
     return b;
 }
+size_t ckpt_bytes(const lbmgpu_handle* h, int n_links) { return ckpt_payload(h->p, n_links); }
+
+void ckpt_fill_deck(CkptHeader& hd, const lbmgpu_params& p) {
+    hd.walls_y = p.walls_y; hd.walls_z = p.walls_z; hd.planar = p.planar;
+    hd.mass_correction_every = p.mass_correction_every; hd.traj_every = p.traj_every; hd.reserved = 0;
+    hd.tau = p.tau; hd.lambda = p.lambda; hd.fx = p.fx; hd.fy = p.fy; hd.fz = p.fz;
+    hd.radius = p.radius; hd.b1 = p.b1; hd.beta = p.beta; hd.rho_p = p.rho_p;
+    hd.eps = p.eps; hd.hc = p.hc; hd.hmin = p.hmin;
+}
+
+// Every check of a checkpoint against the parameters of the lattice it is to
+// be loaded into, on the host. Returns an empty string when it may be loaded.
+std::string ckpt_check(const lbmgpu_params& p, const void* buf, size_t len) {
+    if (!buf) return "null checkpoint buffer";
+    if (len < sizeof(CkptHeader)) return "not a checkpoint (too short)";
+    CkptHeader hd;
+    std::memcpy(&hd, buf, sizeof(hd));
+    if (std::memcmp(hd.magic, CKPT_MAGIC, 8) != 0 || hd.version != CKPT_VERSION)
+        return "not a checkpoint of this library (magic/version)";
+    const size_t N = (size_t)p.nx * p.ny * p.nz;
+    if (hd.nx != p.nx || hd.ny != p.ny || hd.nz != p.nz || (int)hd.precision != p.precision ||
+        hd.has_sq != p.squirmer || hd.sq_bytes != sizeof(SqState) || hd.f_bytes != (uint64_t)Q * N * esize_for(p.precision))
+        return "checkpoint of another lattice (sizes, precision or squirmer differ)";
+    CkptHeader mine{};
+    ckpt_fill_deck(mine, p);
+    const bool same_deck = hd.walls_y == mine.walls_y && hd.walls_z == mine.walls_z &&
+                           hd.mass_correction_every == mine.mass_correction_every && hd.traj_every == mine.traj_every &&
+                           std::memcmp(&hd.tau, &mine.tau, 5 * sizeof(double)) == 0 &&
+                           (!p.squirmer || (hd.planar == mine.planar &&
+                                            std::memcmp(&hd.radius, &mine.radius, 7 * sizeof(double)) == 0));
+    if (!same_deck)
+        return "checkpoint of another deck (walls, tau, lambda, body force, cadences or squirmer model differ)";
+    if (hd.t_main < 0 || hd.traj_read < 0 || (hd.pending_corr != 0 && hd.pending_corr != 1))
+        return "checkpoint header corrupt (counters)";
+    if (hd.n_links < 0 || hd.n_links > (p.squirmer ? link_capacity(p) : 0))
+        return "checkpoint link list too long";
+    if (len < ckpt_payload(p, hd.n_links)) return "checkpoint truncated";
+    // payload: node types against the lattice's wall layers
+    const char* q = static_cast<const char*>(buf) + sizeof(hd) + hd.f_bytes;
+    const uint8_t* flag = reinterpret_cast<const uint8_t*>(q);
+    for (int z = 0; z < p.nz; ++z)
+        for (int y = 0; y < p.ny; ++y) {
+            const bool wall = is_wall(p, y, z), nw = !wall && near_wall(p, y, z);
+            const uint8_t* row = flag + hidx(p, 0, y, z);
+            for (int x = 0; x < p.nx; ++x) {
+                const uint8_t t = row[x] & TYPE_MASK;
+                if (row[x] & ~(uint8_t)(TYPE_MASK | NEAR_WALL | NEAR_PARTICLE) || t > T_PARTICLE)
+                    return "checkpoint corrupt: invalid node flag";
+                if ((t == T_WALL) != wall || ((row[x] & NEAR_WALL) != 0) != nw || (t == T_PARTICLE && !p.squirmer))
+                    return "checkpoint corrupt: node types disagree with the lattice's walls";
+            }
+        }
+    q += N + 4 * N * sizeof(double);
+    SqState s;
+    std::memcpy(&s, q, sizeof(s));
+    q += sizeof(SqState);
+    if (s.status != 0) return "checkpoint of a failed run (device status set)";
+    if (s.t < 0 || s.traj_count < 0 || s.n_fluid < 0 || s.n_fluid > (long long)N)
+        return "checkpoint corrupt: squirmer counters";
+    if (!p.squirmer) return std::string();
+    if (s.n_links != hd.n_links) return "checkpoint corrupt: link count differs between header and state";
+    if (s.R != p.radius || s.B1 != p.b1 || s.beta != p.beta || s.planar != p.planar || s.present != 1)
+        return "checkpoint of another deck (squirmer model differs)";
+    for (int d = 0; d < 3; ++d)
+        if (!std::isfinite(s.X[d]) || !std::isfinite(s.e[d]) || !std::isfinite(s.U[d]) || !std::isfinite(s.W[d]))
+            return "checkpoint corrupt: non-finite squirmer state";
+    // the centre: unwrapped along x (bounded well inside int range), inside
+    // the channel along a walled axis
+    if (std::fabs(s.X[0]) > 1e9 || std::fabs(s.X[1]) > 1e9 || std::fabs(s.X[2]) > 1e9 ||
+        (p.walls_y && (s.X[1] < 0.0 || s.X[1] > p.ny - 1)) || (p.walls_z && (s.X[2] < 0.0 || s.X[2] > p.nz - 1)))
+        return "checkpoint corrupt: squirmer centre outside the lattice";
+    // zone boxes: the widths of this lattice, corners inside the ranges the
+    // zone kernel indexes from (wrapped along periodic axes)
+    const int nd[3] = {p.nx, p.ny, p.nz};
+    const bool wall_axis[3] = {false, p.walls_y != 0, p.walls_z != 0};
+    for (int k = 0; k < ZONE_SLOTS; ++k)
+        for (int d = 0; d < 3; ++d) {
+            const int w = s.zone[k].w[d], lo = s.zone[k].lo[d];
+            if (w != zone_width(p.radius, nd[d], wall_axis[d])) return "checkpoint corrupt: zone width";
+            if (wall_axis[d] ? (lo < -w || lo > nd[d]) : (lo < 0 || lo >= nd[d])) return "checkpoint corrupt: zone corner";
+        }
+    // link nodes: ascending, inside the lattice, FLUID with the near-particle bit
+    const int* links = reinterpret_cast<const int*>(q);
+    for (int k = 0; k < hd.n_links; ++k) {
+        const int n = links[k];
+        if (n < 0 || (size_t)n >= N || (k > 0 && n <= links[k - 1]))
+            return "checkpoint corrupt: link node index out of range or out of order";
+        if (flag[n] != (T_FLUID | NEAR_PARTICLE) && flag[n] != (T_FLUID | NEAR_PARTICLE | NEAR_WALL))
+            return "checkpoint corrupt: link node is not a fluid node next to the sphere";
+    }
+    return std::string();
+}
+
 int ckpt_links(lbmgpu_handle* h, int* n_links) {
     SqState s;
     CUDA_TRY(h, cudaMemcpyAsync(&s, h->sq, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
@@ -1003,11 +1228,12 @@ int lbmgpu_checkpoint_save(lbmgpu_handle* h, void* buf, size_t len) {
     const size_t N = h->L.N;
     CkptHeader hd{};
     std::memcpy(hd.magic, CKPT_MAGIC, 8);
-    hd.version = 1; hd.precision = (uint32_t)h->p.precision;
+    hd.version = CKPT_VERSION; hd.precision = (uint32_t)h->p.precision;
     hd.nx = h->p.nx; hd.ny = h->p.ny; hd.nz = h->p.nz; hd.has_sq = h->has_sq;
     hd.t_main = h->t_main; hd.traj_read = h->traj_read; hd.pending_corr = h->pending_corr ? 1 : 0;
     hd.n_links = nl;
     hd.f_bytes = (uint64_t)Q * N * h->esize; hd.sq_bytes = sizeof(SqState);
+    ckpt_fill_deck(hd, h->p);
     char* p = static_cast<char*>(buf);
     std::memcpy(p, &hd, sizeof(hd)); p += sizeof(hd);
     cudaStream_t st = h->stream;
@@ -1034,17 +1260,10 @@ int lbmgpu_checkpoint_save(lbmgpu_handle* h, void* buf, size_t len) {
 int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len) {
     if (!h || !buf) return LBMGPU_ERR_INVALID;
     if (h->member) return fail(h, LBMGPU_ERR_INVALID, "handle belongs to an ensemble: advance it with lbmgpu_batch_run");
-    if (len < sizeof(CkptHeader)) return fail(h, LBMGPU_ERR_INVALID, "not a checkpoint (too short)");
+    const std::string why = ckpt_check(h->p, buf, len);
+    if (!why.empty()) return fail(h, LBMGPU_ERR_INVALID, why);
     CkptHeader hd;
     std::memcpy(&hd, buf, sizeof(hd));
-    if (std::memcmp(hd.magic, CKPT_MAGIC, 8) != 0 || hd.version != 1)
-        return fail(h, LBMGPU_ERR_INVALID, "not a checkpoint of this library (magic/version)");
-    if (hd.nx != h->p.nx || hd.ny != h->p.ny || hd.nz != h->p.nz || (int)hd.precision != h->p.precision ||
-        hd.has_sq != h->has_sq || hd.sq_bytes != sizeof(SqState) ||
-        hd.f_bytes != (uint64_t)Q * h->L.N * h->esize)
-        return fail(h, LBMGPU_ERR_INVALID, "checkpoint of another lattice (sizes, precision or squirmer differ)");
-    if (hd.n_links < 0 || hd.n_links > h->link_cap) return fail(h, LBMGPU_ERR_INVALID, "checkpoint link list too long");
-    if (len < ckpt_bytes(h, hd.n_links)) return fail(h, LBMGPU_ERR_INVALID, "checkpoint truncated");
     CUDA_TRY(h, cudaSetDevice(h->p.device));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (h->zs) CUDA_TRY(h, cudaStreamSynchronize(h->zs));
@@ -1070,6 +1289,10 @@ int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len) {
             ++h->launches;
         }
         CUDA_TRY(h, h2d(h->traj, (size_t)TRAJ_RING * TRAJ_COLS * sizeof(double)));
+        // the cached remap shell belongs to this handle's earlier state: rebuild
+        // it from the loaded centre (its content never changes results, only
+        // which candidates are tested)
+        CUDA_TRY(h, cudaMemsetAsync(h->shell_hdr, 0, sizeof(ShellCache), st));
     }
     CUDA_TRY(h, cudaStreamSynchronize(st));
     CUDA_TRY(h, cudaGetLastError());
@@ -1077,6 +1300,17 @@ int lbmgpu_checkpoint_load(lbmgpu_handle* h, const void* buf, size_t len) {
     h->traj_read = hd.traj_read;
     h->pending_corr = hd.pending_corr != 0;
     return LBMGPU_OK;
+}
+
+int lbmgpu_checkpoint_check(const lbmgpu_params* p, const void* buf, size_t len, char* msg, size_t msg_len) {
+    std::string m;
+    int rc = validate_impl(p, m);
+    if (rc == LBMGPU_OK) {
+        m = ckpt_check(*p, buf, len);
+        rc = m.empty() ? LBMGPU_OK : LBMGPU_ERR_INVALID;
+    }
+    if (msg && msg_len) std::snprintf(msg, msg_len, "%s", m.c_str());
+    return rc;
 }
 
 int lbmgpu_get_populations(lbmgpu_handle* h, double* f) {
@@ -1894,20 +2128,47 @@ __global__ void __launch_bounds__(STATS_BLOCK) k_field_stats_static(unsigned lon
     }
 }
 
-// Device address of g_stats_scratch, looked up once per device.
+// Device address of g_stats_scratch, looked up once per device and context.
+// The address belongs to the device's (primary) context: after the context is
+// destroyed and recreated (cudaDeviceReset) the module is loaded again and the
+// array may live elsewhere, so the cache entry is keyed by the context that
+// was current at the lookup (the driver's cuCtxGetCurrent, reached through
+// the runtime's cudaGetDriverEntryPoint, so no link against libcuda is needed).
 constexpr int STATS_MAX_DEVICES = 64;
 std::mutex g_stats_mu;
-StatsScratch* g_stats_addr[STATS_MAX_DEVICES] = {};
+struct StatsAddr {
+    void* ctx;
+    StatsScratch* addr;
+};
+StatsAddr g_stats_addr[STATS_MAX_DEVICES] = {};
+
+using CtxGetCurrentFn = int (*)(void**);   // CUresult cuCtxGetCurrent(CUcontext*)
+void* current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 cudaError_t stats_scratch(int dev, StatsScratch** out) {
     std::lock_guard<std::mutex> lk(g_stats_mu);
-    if (!g_stats_addr[dev]) {
+    StatsAddr& c = g_stats_addr[dev];
+    void* ctx = current_context();
+    if (!c.addr || !ctx || ctx != c.ctx) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_stats_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_stats_scratch);   // binds the device's context
         if (e != cudaSuccess) return e;
-        g_stats_addr[dev] = static_cast<StatsScratch*>(p);
+        c.addr = static_cast<StatsScratch*>(p);
+        c.ctx = current_context();
     }
-    *out = g_stats_addr[dev];
+    *out = c.addr;
     return cudaSuccess;
 }
 

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <fstream>
+#include <future>
 #include <iterator>
 #include <memory>
 #include <stdexcept>
@@ -56,6 +57,47 @@ struct Device {
     }
 };
 
+// VTK snapshots written beside the time loop: the device packs the fields of
+// the snapshot step into a buffer of its own (lbmgpu_snapshot_begin) and the
+// loop goes on; a writer thread copies them into page-locked host buffers
+// (lbmgpu_snapshot_read) and writes the file. One snapshot is in flight at a
+// time: the next one first waits for the previous file.
+class SnapshotWriter {
+public:
+    SnapshotWriter(const Device& dev, const Params& p) : dev_(dev) {
+        view_.nx = p.NX; view_.ny = p.NY; view_.nz = p.NZ;
+        const size_t N = view_.size();
+        flag_ = static_cast<uint8_t*>(lbmgpu_host_alloc(N));
+        rho_ = static_cast<double*>(lbmgpu_host_alloc(N * sizeof(double)));
+        u_ = static_cast<double*>(lbmgpu_host_alloc(3 * N * sizeof(double)));
+        if (!flag_ || !rho_ || !u_) throw std::runtime_error("cannot allocate page-locked snapshot buffers");
+        view_.flag = flag_; view_.rho = rho_; view_.u = u_;
+    }
+    ~SnapshotWriter() {
+        if (pending_.valid()) pending_.wait();
+        lbmgpu_host_free(flag_); lbmgpu_host_free(rho_); lbmgpu_host_free(u_);
+    }
+    void write(const std::string& path) {
+        finish();
+        dev_.check(lbmgpu_snapshot_begin(dev_.h));
+        pending_ = std::async(std::launch::async, [this, path] {
+            if (lbmgpu_snapshot_read(dev_.h, flag_, rho_, u_) != LBMGPU_OK)
+                throw std::runtime_error(std::string("device: ") + lbmgpu_snapshot_last_error(dev_.h));
+            writeVtk(view_, path);
+        });
+    }
+    void finish() {   // rethrows a failure of the previous write
+        if (pending_.valid()) pending_.get();
+    }
+private:
+    const Device& dev_;
+    FieldsView view_;
+    uint8_t* flag_ = nullptr;
+    double* rho_ = nullptr;
+    double* u_ = nullptr;
+    std::future<void> pending_;
+};
+
 void drainTrajectory(const Device& dev, TrajectoryFile& traj) {
     static double rows[1024 * 15];
     for (;;) {
@@ -93,6 +135,9 @@ int runSimulation(const Params& p) {
     if (p.squirmer) traj = std::make_unique<TrajectoryFile>(base + "_traj.dat", !p.restart.empty());
     const double nu = (p.tau - 0.5) / 3.0;
 
+    std::unique_ptr<SnapshotWriter> snaps;
+    if (p.vtkEvery > 0) snaps = std::make_unique<SnapshotWriter>(dev, p);
+
     const auto t0 = std::chrono::steady_clock::now();
     double prevSum = 0.0;
     bool converged = false;
@@ -106,7 +151,7 @@ int runSimulation(const Params& p) {
         dev.check(lbmgpu_run(dev.h, (int)(next - t)));
         t = (int)next;
         if (p.squirmer) drainTrajectory(dev, *traj);
-        if (p.vtkEvery > 0 && t % p.vtkEvery == 0) writeVtk(dev.fields(p), base + "_" + std::to_string(t) + ".vtk");
+        if (snaps && t % p.vtkEvery == 0) snaps->write(base + "_" + std::to_string(t) + ".vtk");
         if (p.checkpointEvery > 0 && t % p.checkpointEvery == 0) {
             if (traj) traj->flush();
             size_t n = 0;
@@ -139,6 +184,7 @@ int runSimulation(const Params& p) {
             std::fflush(stdout);
         }
     }
+    if (snaps) snaps->finish();
     const int done = converged ? t : p.steps;
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     const double ncell = (double)p.NX * p.NY * p.NZ;

@@ -36,14 +36,14 @@ void makeDirectory(const std::string& dir) {
 
 // io.cpp:44-67: flag (u8), density (f64; 1 on solid nodes), velocity
 // (3 x f64; 0 on solid nodes), STRUCTURED_POINTS with unit spacing.
-void writeVtk(const Fields& F, const std::string& path) {
+void writeVtk(const FieldsView& F, const std::string& path) {
     std::FILE* fp = std::fopen(path.c_str(), "wb");
     if (!fp) throw std::runtime_error("cannot write '" + path + "'");
     const size_t N = F.size();
     std::fprintf(fp, "# vtk DataFile Version 3.0\nlbm-squirmer\nBINARY\nDATASET STRUCTURED_POINTS\n");
     std::fprintf(fp, "DIMENSIONS %d %d %d\nORIGIN 0 0 0\nSPACING 1 1 1\nPOINT_DATA %zu\n", F.nx, F.ny, F.nz, N);
     std::fprintf(fp, "SCALARS flag unsigned_char 1\nLOOKUP_TABLE default\n");
-    std::fwrite(F.flag.data(), 1, N, fp);
+    std::fwrite(F.flag, 1, N, fp);
     std::fprintf(fp, "\n");
     std::vector<double> d(N);
     for (size_t n = 0; n < N; ++n) d[n] = F.flag[n] == LBMGPU_FLUID ? F.rho[n] : 1.0;

@@ -18,16 +18,27 @@
 
 namespace lbmdrv {
 
+// The fields the writers read, wherever they live.
+struct FieldsView {
+    int nx = 0, ny = 0, nz = 0;
+    const uint8_t* flag = nullptr;
+    const double* rho = nullptr;
+    const double* u = nullptr;   // interleaved (ux, uy, uz)
+    size_t size() const { return (size_t)nx * ny * nz; }
+};
+
 // Host copy of the fields the writers need.
 struct Fields {
     int nx = 0, ny = 0, nz = 0;
     std::vector<uint8_t> flag;
     std::vector<double> rho, u;  // u interleaved (ux, uy, uz)
     size_t size() const { return (size_t)nx * ny * nz; }
+    FieldsView view() const { return FieldsView{nx, ny, nz, flag.data(), rho.data(), u.data()}; }
 };
 
 void makeDirectory(const std::string& dir);                  // throws std::runtime_error
-void writeVtk(const Fields& F, const std::string& path);     // throws std::runtime_error
+void writeVtk(const FieldsView& F, const std::string& path); // throws std::runtime_error
+inline void writeVtk(const Fields& F, const std::string& path) { writeVtk(F.view(), path); }
 
 class TrajectoryFile {
 public:

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import LbmgpuDiagnostics, LbmgpuSquirmer, check, dptr, u8ptr
+from ._lib import LBMGPU_OK, LbmgpuDiagnostics, LbmgpuSquirmer, check, dptr, load, u8ptr
 from .params import Params
 
 Q = 19
@@ -103,6 +103,24 @@ class Solver:
         check(self.lib.lbmgpu_fields(self.h, u8ptr(flag), dptr(rho), dptr(u)), self.h)
         return flag.reshape(self.shape), rho.reshape(self.shape), u.reshape(self.shape + (3,))
 
+    def snapshot_begin(self) -> None:
+        """Queue a device-side copy of the last step's fields (lbmgpu_snapshot_begin);
+        the time loop may continue before it is read."""
+        check(self.lib.lbmgpu_snapshot_begin(self.h), self.h)
+
+    def snapshot_read(self, out: "HostFields | None" = None):
+        """The fields of the last snapshot (lbmgpu_snapshot_read), as fields() returns them."""
+        out = out or HostFields(self.N)
+        rc = self.lib.lbmgpu_snapshot_read(self.h, u8ptr(out.flag), dptr(out.rho), dptr(out.u))
+        if rc != LBMGPU_OK:
+            raise _lib.LbmgpuError(rc, self.lib.lbmgpu_snapshot_last_error(self.h).decode())
+        return out.shaped(self.shape)
+
+    def fields_into(self, out: "HostFields"):
+        """fields() into caller-owned (e.g. page-locked) host buffers."""
+        check(self.lib.lbmgpu_fields(self.h, u8ptr(out.flag), dptr(out.rho), dptr(out.u)), self.h)
+        return out.shaped(self.shape)
+
     def diag(self) -> dict:
         d = LbmgpuDiagnostics()
         check(self.lib.lbmgpu_diag(self.h, ctypes.byref(d)), self.h)
@@ -144,6 +162,16 @@ class Solver:
         """Continue from a checkpoint of a lattice with the same parameters."""
         check(self.lib.lbmgpu_checkpoint_load(self.h, data, len(data)), self.h)
 
+    @staticmethod
+    def check_checkpoint(p, data: bytes):
+        """None if `data` may be loaded into a lattice with parameters `p`, else
+        the reason (lbmgpu_checkpoint_check: host only, no device, no handle)."""
+        lib = load()
+        msg = ctypes.create_string_buffer(256)
+        c = p.to_c()
+        rc = lib.lbmgpu_checkpoint_check(ctypes.byref(c), data, len(data), msg, 256)
+        return None if rc == LBMGPU_OK else msg.value.decode()
+
     def save(self, path) -> None:
         with open(path, "wb") as fh:
             fh.write(self.checkpoint())
@@ -169,3 +197,44 @@ class Solver:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class HostFields:
+    """Host buffers for the fields of an N-node lattice (node types, rho, u
+    interleaved). pinned=True places them in page-locked memory
+    (lbmgpu_host_alloc), which the device copies into directly."""
+
+    def __init__(self, n: int, pinned: bool = False):
+        self.n = n
+        self._ptrs = []
+        if pinned:
+            lib = load()
+
+            def alloc(count, ctype):
+                p = lib.lbmgpu_host_alloc(count * ctypes.sizeof(ctype))
+                if not p:
+                    raise MemoryError("lbmgpu_host_alloc failed")
+                self._ptrs.append(p)
+                return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctype)), shape=(count,))
+            self.flag = alloc(n, ctypes.c_uint8)
+            self.rho = alloc(n, ctypes.c_double)
+            self.u = alloc(3 * n, ctypes.c_double)
+        else:
+            self.flag = np.empty(n, np.uint8)
+            self.rho = np.empty(n)
+            self.u = np.empty(3 * n)
+
+    def shaped(self, shape):
+        return self.flag.reshape(shape), self.rho.reshape(shape), self.u.reshape(shape + (3,))
+
+    def close(self) -> None:
+        lib = load() if self._ptrs else None
+        for p in self._ptrs:
+            lib.lbmgpu_host_free(p)
+        self._ptrs = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -70,10 +70,44 @@ def ref_available() -> bool:
     return (REF_DIR / "libref_harness.so").exists()
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        path = REF_DIR / "libref_harness.so"
+def _cpu_has_avx512() -> bool:
+    try:
+        flags = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+        return {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags
+    except OSError:
+        return False
+
+
+def timed_build() -> Path:
+    """The build of the reference used for timing: the reference Makefile's
+    flags (-O3 -std=c++17 -fopenmp) at the highest x86-64 level this CPU runs
+    (what -march=native would choose among the levels built), else the parity
+    build."""
+    for name, ok in (("libref_harness_timed_v4.so", _cpu_has_avx512()), ("libref_harness_timed_v3.so", True)):
+        if ok and (REF_DIR / name).exists():
+            return REF_DIR / name
+    return REF_DIR / "libref_harness.so"
+
+
+def ref_build() -> str:
+    """Which compiled reference the timed CPU legs load."""
+    name = timed_build().name
+    return {"libref_harness_timed_v4.so": "reference sources, -O3 -march=x86-64-v4 -std=c++17 -fopenmp",
+            "libref_harness_timed_v3.so": "reference sources, -O3 -march=x86-64-v3 -std=c++17 -fopenmp",
+            }.get(name, "reference sources, parity build -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp")
+
+
+_ref_timed = None
+
+
+def ref_lib(timed: bool = False):
+    global _ref, _ref_timed
+    if (_ref_timed if timed else _ref) is None:
+        path = timed_build() if timed else REF_DIR / "libref_harness.so"
         if not path.exists():
             raise RuntimeError(f"{path} missing: run make -C oracle (needs the reference sources)")
         lib = ctypes.CDLL(str(path))
@@ -95,8 +129,11 @@ def ref_lib():
         lib.ref_poiseuille_error.argtypes = [_P, ctypes.c_char_p]; lib.ref_poiseuille_error.restype = _D
         lib.ref_duct_velocity.argtypes = [_D] * 6; lib.ref_duct_velocity.restype = _D
         lib.ref_write_vtk.argtypes = [_P, ctypes.c_char_p]
-        _ref = lib
-    return _ref
+        if timed:
+            _ref_timed = lib
+        else:
+            _ref = lib
+    return _ref_timed if timed else _ref
 
 
 class _Solver:
@@ -193,11 +230,13 @@ class PortSolver(_Solver):
 
 
 class RefSolver(_Solver):
-    """The reference's own code (compiled from its sources by oracle/Makefile)."""
+    """The reference's own code (compiled from its sources by oracle/Makefile).
+    timed=True loads the build with the reference Makefile's own flags (for
+    the CPU baseline); the default is the parity build."""
 
-    def __init__(self, params):
+    def __init__(self, params, timed: bool = False):
         super().__init__(params)
-        lib = self.lib = ref_lib()
+        lib = self.lib = ref_lib(timed)
         kv = [s.encode() for s in params.to_kv(reference_only=True)]
         arr = (ctypes.c_char_p * len(kv))(*kv)
         err = ctypes.create_string_buffer(512)

@@ -1,8 +1,8 @@
 """Collect the reference's shipped result files into tests/golden/shipped.npz.
 
-    python tests/golden/extract_shipped.py [REFERENCE_ROOT]
+    python tests/golden/extract_shipped.py REFERENCE_ROOT
 
-Reads (from the reference checkout, default /root/reference):
+Reads (from the reference checkout given as the argument):
   outputs/duct_summary.txt, outputs/duct_profile_{y,z}.dat
   outputs/channel_{neutral,puller,pusher}_{summary.txt,squirmer.dat}
   outputs/channel_puller_traj.dat
@@ -30,7 +30,9 @@ def keyvalue(path: Path) -> dict:
 
 
 def main() -> None:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/extract_shipped.py REFERENCE_ROOT")
+    ref = Path(sys.argv[1])
     arrays = {}
     for name in ("duct", "channel_neutral", "channel_puller", "channel_pusher"):
         for k, v in keyvalue(ref / "outputs" / f"{name}_summary.txt").items():

@@ -9,6 +9,9 @@ writes tests/golden/ref_<case>.npz with
   * the trajectory rows (the columns of the reference's _traj.dat),
   * the final squirmer state and diagnostics (countFluid/meanDensity/...),
   * rho, u and flag at a fixed seeded sample of nodes (4096, rng seed 7),
+  * with a squirmer: rho, u and flag at every node of the sphere's shell,
+    i.e. within R + SHELL_PAD of the final centre (minimum image), where the
+    moving boundary, the refill and any precision effects concentrate,
   * for the duct: the whole x=0 cross-section,
   * wall-clock seconds and the OpenMP thread count used.
 With --full-dir the complete final fields are also written there as .npy
@@ -36,6 +39,21 @@ from oracle.oracle import RefSolver, set_threads  # noqa: E402
 CASES = ("duct", "slit", "bulk_m3", "bulk_0", "bulk_p3")
 SAMPLE_SEED = 7
 SAMPLE_SIZE = 4096
+SHELL_PAD = 3.0
+
+
+def shell_nodes(p: Params, X: np.ndarray) -> np.ndarray:
+    """Node indices (ascending) within R + SHELL_PAD of centre X, with the
+    minimum image along every periodic axis."""
+    z, y, x = np.meshgrid(np.arange(p.NZ), np.arange(p.NY), np.arange(p.NX), indexing="ij")
+    d = []
+    for c, n, periodic in ((x, p.NX, True), (y, p.NY, not p.wallsY), (z, p.NZ, not p.wallsZ)):
+        r = c - X[len(d)]
+        if periodic:
+            r = r - n * np.round(r / n)
+        d.append(r)
+    r2 = d[0] ** 2 + d[1] ** 2 + d[2] ** 2
+    return np.flatnonzero((r2 < (p.R + SHELL_PAD) ** 2).reshape(-1))
 
 
 def sample_nodes(n_cells: int) -> np.ndarray:
@@ -77,6 +95,9 @@ def main() -> None:
         for k in ("X", "e", "U", "W", "Fh", "Th", "Fc", "Tc", "Fw"):
             out["sq_" + k] = sq[k]
         out["sq_contacts"] = sq["contacts"]
+        sh = shell_nodes(p, np.asarray(sq["X"]))
+        out.update(shell_idx=sh, shell_flag=flag.reshape(-1)[sh], shell_rho=rho.reshape(-1)[sh],
+                   shell_u=u.reshape(-1, 3)[sh])
     if a.case == "duct":
         out["x0_rho"] = rho[:, :, 0]
         out["x0_u"] = u[:, :, 0, :]

@@ -115,3 +115,14 @@ def test_static_stats_checks_arguments_before_touching_the_device():
     for n in (0, -5, (1 << 25) + 1):
         assert lib.lbmgpu_field_stats_static(fake, fake, fake, fake, fake, n, None, ctypes.byref(d)) == -1
         assert b"33554432, the capacity of its static scratch" in lib.lbmgpu_last_error(None)
+
+
+def test_checkpoint_check_rejects_garbage_without_a_device():
+    """lbmgpu_checkpoint_check validates a restart buffer against parameters on
+    the host alone: no handle, no device."""
+    from lbm_solver_3d_b200.solver import Solver
+    p = Params().update(nx=40, ny=26, nz=22, squirmer=1, radius=4.5)
+    assert "not a checkpoint" in Solver.check_checkpoint(p, b"x" * 400)
+    assert "too short" in Solver.check_checkpoint(p, b"LBMGPUCK")
+    bad = Params().update(nx=0)
+    assert "grid dimensions" in Solver.check_checkpoint(bad, b"x" * 400)

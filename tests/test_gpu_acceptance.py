@@ -1,0 +1,209 @@
+"""The reference's acceptance suite, restated against the GPU drop-in.
+
+The reference validates its solver with pytest checks on the files its
+executable writes (tests/test_duct_flow.py and tests/test_squirmer_bulk.py in
+the reference). The same physics checks run here through the drop-in
+executable lbm_squirmer_gpu, with the same decks and the same bounds, in the
+plain FP64 method and in the FP32-shifted form (and, for the squirmer, the
+FP16-storage form): they are the forms' checks against physics rather than
+against FP64.
+
+Then the drop-in's result files are compared with the reference executable's
+(oracle/_ref/lbm_squirmer_ref, built from the reference's own sources) on the
+same decks: VTK headers and node types exactly, density and velocity, the
+summary, squirmer state, trajectory and Poiseuille profile files value by
+value.
+"""
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from lbm_files import near_field_error, read_keyvalue, read_traj, read_vtk
+
+pytestmark = pytest.mark.gpu
+DRIVER = ROOT / "lbm_solver_3d_b200" / "bin" / "lbm_squirmer_gpu"
+REF_EXE = ROOT / "oracle" / "_ref" / "lbm_squirmer_ref"
+
+# the reference's decks (inputs/duct.in, inputs/bulk_squirmer.in) as keys
+DUCT = dict(nx=4, ny=34, nz=34, tau=0.8, fx=5e-5, walls_y=1, walls_z=1, squirmer=0, steps=100000, tol=1e-12,
+            print_every=1000)
+BULK = dict(nx=48, ny=48, nz=48, tau=1.0, walls_y=0, walls_z=0, squirmer=1, radius=4, b1=0.015, beta=0, angle=0,
+            planar=1, steps=3000, print_every=500, traj_every=10)
+CHANNEL = dict(nx=64, ny=34, nz=32, tau=1.0, walls_y=1, walls_z=0, squirmer=1, radius=4, b1=0.015, beta=0,
+               angle=30, planar=1, eps=0.2, hc=2.0, hmin=0.5, print_every=300, traj_every=50)
+WIDTHS = (8, 16, 32)
+
+
+def run(exe, outdir, deck, **kw):
+    args = [str(exe), "/dev/null"] + [f"{k}={v}" for k, v in {**deck, **kw}.items()] + [f"output_dir={outdir}"]
+    res = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout + res.stderr
+    return res.stdout
+
+
+# ---- test_duct_flow.py (the reference's) ----------------------------------
+@pytest.fixture(scope="module", params=["fp64", "fp32"])
+def duct_runs(request, tmp_path_factory):
+    prec = request.param
+    out = tmp_path_factory.mktemp(f"duct_{prec}")
+    runs = {}
+    for H in WIDTHS:
+        fx = 5e-5 * (32 / H) ** 2   # u_max, hence Re and Ma, fixed across H
+        run(DRIVER, out, DUCT, ny=H + 2, nz=H + 2, fx=fx, prefix=f"duct_H{H}", precision=prec)
+        runs[H] = read_keyvalue(out / f"duct_H{H}_summary.txt")
+    return prec, runs
+
+
+def test_duct_matches_exact_solution(duct_runs):
+    prec, runs = duct_runs
+    s = runs[32]
+    if prec == "fp64":   # FP32 rounding noise keeps the relative change above 1e-12
+        assert s["converged"][0] == 1
+    assert s["l2_error"][0] < 5e-4, f"{prec}: L2 error {s['l2_error'][0]:.2e}"
+
+
+def test_duct_second_order_convergence(duct_runs):
+    prec, runs = duct_runs
+    err = np.array([runs[H]["l2_error"][0] for H in WIDTHS])
+    order = np.log(err[:-1] / err[1:]) / np.log(2)
+    print(f"{prec}: L2 errors {err}, orders {order}")
+    assert np.all(order > 1.8), f"{prec}: observed orders {order}"
+
+
+def test_duct_momentum_balance_and_mass(duct_runs):
+    prec, runs = duct_runs
+    for H, s in runs.items():
+        fw, fb = s["wall_force"][0], s["body_force_total"][0]
+        assert abs(fw - fb) / fb < 1e-6, f"{prec} H={H}: wall force {fw} vs body force {fb}"
+        assert abs(s["mean_density"][0] - 1.0) < 1e-10
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_plane_channel(prec, tmp_path):
+    """Walls in y only: TRT with Lambda = 3/16 is exact for plane Poiseuille flow."""
+    run(DRIVER, tmp_path, DUCT, nx=4, ny=34, nz=1, walls_z=0, tau=0.8, fx=1e-5, prefix="plane", precision=prec)
+    s = read_keyvalue(tmp_path / "plane_summary.txt")
+    print(f"{prec}: plane channel L2 {s['l2_error'][0]:.2e}")
+    assert s["l2_error"][0] < 1e-6
+
+
+# ---- test_squirmer_bulk.py (the reference's) --------------------------------
+BETAS = (-3, 0, 3)
+
+
+@pytest.fixture(scope="module", params=["fp64", "fp32", "fp16"])
+def bulk_runs(request, tmp_path_factory):
+    prec = request.param
+    out = tmp_path_factory.mktemp(f"bulk_{prec}")
+    runs = {}
+    for beta in BETAS:
+        prefix = f"bulk_beta{beta:+d}"
+        run(DRIVER, out, BULK, nx=40, ny=40, nz=40, beta=beta, steps=2000, prefix=prefix, precision=prec)
+        runs[beta] = dict(traj=read_traj(out / f"{prefix}_traj.dat"),
+                          state=read_keyvalue(out / f"{prefix}_squirmer.dat"),
+                          summary=read_keyvalue(out / f"{prefix}_summary.txt"),
+                          vtk=read_vtk(out / f"{prefix}_final.vtk"))
+    return prec, runs
+
+
+U0 = 2 * 0.015 / 3
+
+
+def late(tr, key):
+    return tr[key][tr["t"] > 1000]
+
+
+def test_neutral_swimming_speed(bulk_runs):
+    prec, runs = bulk_runs
+    ratio = late(runs[0]["traj"], "Ux").mean() / U0
+    print(f"{prec}: <Ux>/U0 = {ratio:.4f}")
+    assert 0.93 < ratio < 1.03
+
+
+def test_straight_swimming(bulk_runs):
+    prec, runs = bulk_runs
+    for beta, r in runs.items():
+        tr = r["traj"]
+        assert np.abs(late(tr, "Uy")).max() < 1e-3 * U0, f"{prec} beta={beta}: lateral drift"
+        assert np.abs(late(tr, "Wz")).max() < 1e-6, f"{prec} beta={beta}: rotation"
+        assert np.abs(tr["angle"]).max() < 1e-6
+
+
+def test_finite_reynolds_speed_ordering(bulk_runs):
+    prec, runs = bulk_runs
+    u = {b: late(r["traj"], "Ux").mean() for b, r in runs.items()}
+    assert u[-3] > u[0] > u[3], f"{prec}: speeds {u}"
+
+
+def test_mass_conservation(bulk_runs):
+    prec, runs = bulk_runs
+    for beta, r in runs.items():
+        assert abs(r["summary"]["mean_density"][0] - 1.0) < 1e-4
+
+
+def test_flow_field_matches_blake(bulk_runs):
+    """Near field (1.25R < r < 3R, the lattice plane through the centre) within
+    30 % of the unbounded Blake solution: a regression bound (staircase sphere
+    of R = 4, periodic images, Re ~ 0.5), as in the reference."""
+    prec, runs = bulk_runs
+    for beta, r in runs.items():
+        e = near_field_error(r["vtk"], r["state"]["X"], 4.0, 0.015, beta)
+        print(f"{prec} beta={beta}: near-field error {e:.3f}")
+        assert e < 0.30
+
+
+# ---- result files of the drop-in against the reference executable's ---------
+def _ref_exe():
+    if not REF_EXE.exists():
+        pytest.skip("reference executable not built (needs the reference sources)")
+    return REF_EXE
+
+
+def _compare_vtk(a_path, b_path):
+    a, b = read_vtk(a_path), read_vtk(b_path)
+    assert a["header"] == b["header"]
+    assert np.array_equal(a["flag"], b["flag"])
+    for k in ("density", "velocity"):
+        d = np.abs(a[k] - b[k]).max()
+        scale = max(np.abs(b[k]).max(), 1e-300)
+        assert d <= 1e-10 * scale, f"{a_path.name} {k}: max diff {d:.2e} (scale {scale:.2e})"
+
+
+def _compare_keyvalue(a_path, b_path, rtol=1e-9, atol=1e-15):
+    a, b = read_keyvalue(a_path), read_keyvalue(b_path)
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.allclose(a[k], b[k], rtol=rtol, atol=atol), f"{a_path.name} {k}: {a[k]} vs {b[k]}"
+
+
+def test_result_files_equal_the_reference_duct(tmp_path):
+    ref = _ref_exe()
+    deck = dict(DUCT, ny=18, nz=18, fx=2e-4, steps=3000, tol=0, vtk_every=1000, prefix="duct")
+    (tmp_path / "gpu").mkdir(); (tmp_path / "ref").mkdir()
+    run(DRIVER, tmp_path / "gpu", deck)
+    run(ref, tmp_path / "ref", deck)
+    for name in ("duct_1000.vtk", "duct_2000.vtk", "duct_3000.vtk", "duct_final.vtk"):
+        _compare_vtk(tmp_path / "gpu" / name, tmp_path / "ref" / name)
+    _compare_keyvalue(tmp_path / "gpu" / "duct_summary.txt", tmp_path / "ref" / "duct_summary.txt")
+    for name in ("duct_profile_y.dat", "duct_profile_z.dat"):
+        a, b = np.loadtxt(tmp_path / "gpu" / name), np.loadtxt(tmp_path / "ref" / name)
+        assert a.shape == b.shape and np.allclose(a, b, rtol=1e-9, atol=1e-15)
+
+
+def test_result_files_equal_the_reference_channel(tmp_path):
+    ref = _ref_exe()
+    deck = dict(CHANNEL, steps=600, vtk_every=300, prefix="channel")
+    (tmp_path / "gpu").mkdir(); (tmp_path / "ref").mkdir()
+    run(DRIVER, tmp_path / "gpu", deck)
+    run(ref, tmp_path / "ref", deck)
+    for name in ("channel_300.vtk", "channel_600.vtk", "channel_final.vtk"):
+        _compare_vtk(tmp_path / "gpu" / name, tmp_path / "ref" / name)
+    _compare_keyvalue(tmp_path / "gpu" / "channel_summary.txt", tmp_path / "ref" / "channel_summary.txt")
+    _compare_keyvalue(tmp_path / "gpu" / "channel_squirmer.dat", tmp_path / "ref" / "channel_squirmer.dat")
+    a = (tmp_path / "gpu" / "channel_traj.dat").read_text().splitlines()
+    b = (tmp_path / "ref" / "channel_traj.dat").read_text().splitlines()
+    assert a[0] == b[0] and len(a) == len(b)
+    ta, tb = np.loadtxt(a[1:]), np.loadtxt(b[1:])
+    assert np.allclose(ta, tb, rtol=1e-9, atol=2e-6)   # %.6f / %.6e columns: last printed digit

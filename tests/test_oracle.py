@@ -131,3 +131,22 @@ def test_port_matches_full_duct_fixture(port):
     assert np.allclose(rho[:, :, 0], g["x0_rho"], rtol=1e-13, atol=0)
     assert np.allclose(u[:, :, 0], g["x0_u"], rtol=1e-9, atol=1e-18)
     assert abs(s.poiseuille_error() - float(g["l2_error"])) < 1e-12
+
+
+def test_timed_reference_build_computes_the_parity_build(oracle_mod):
+    """The CPU baseline loads the reference compiled with its Makefile's own
+    flags at this CPU's x86-64 level. GCC contracts multiply-adds there (its
+    C++ default), so it matches the parity build to rounding: the same
+    solver, timed as its author builds it."""
+    if not oracle_mod.ref_available():
+        pytest.skip("reference harness not built (needs the reference sources)")
+    oracle_mod.set_threads(1)
+    p = deck(CHANNEL, nx=24, ny=18, nz=16, radius=3.5, beta=1.5, angle=10, traj_every=10)
+    a, b = oracle_mod.RefSolver(p), oracle_mod.RefSolver(p, timed=True)
+    ra, rb = a.run(60), b.run(60)
+    assert ra.shape == rb.shape == (6, 15)
+    assert np.allclose(ra, rb, rtol=1e-10, atol=1e-14)
+    fa, fb = a.get_f(), b.get_f()
+    assert np.abs(fa - fb).max() <= 1e-13
+    assert "reference sources" in oracle_mod.ref_build()
+    a.close(); b.close()

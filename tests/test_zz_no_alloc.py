@@ -72,6 +72,32 @@ def test_static_stats_match_diag_two_calls_in_a_row(deck):
     s.close()
 
 
+def test_static_stats_allocates_no_device_memory():
+    """The property the entry point exists for: after one warm-up call (which
+    may load the kernel's module and look up the scratch's address), further
+    calls leave the device's free memory (cudaMemGetInfo) unchanged."""
+    import torch
+    from lbm_solver_3d_b200 import _lib
+    from lbm_solver_3d_b200.solver import Solver
+    lib = _lib.load()
+    p = Params().update(nx=40, ny=26, nz=22, tau=1.0, walls_y=1, squirmer=1, radius=4.5, b1=0.015, angle=20)
+    p.validate()
+    s = Solver(p)
+    s.run(30)
+    dev, _ = device_fields(s)
+    stream = torch.cuda.Stream()
+    first = stats_static(lib, dev, p.ncells, stream.cuda_stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        r = stats_static(lib, dev, p.ncells, stream.cuda_stream)
+        assert r["n_fluid"] == first["n_fluid"] and r["sum_ux"] == first["sum_ux"]
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes across 5 calls"
+    s.close()
+
+
 def test_static_stats_rejects_sizes_beyond_its_scratch():
     from lbm_solver_3d_b200 import _lib
     from lbm_solver_3d_b200._lib import LbmgpuDiagnostics
