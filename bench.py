@@ -427,10 +427,12 @@ def e2e_record(p, args):
     """The metric end to end through the C ABI with host buffers: create the
     lattice from host parameters (flags and boundary links built and copied
     to the device), run K steps in chunks reading the trajectory rows back,
-    then copy the final node types, density and velocity to host memory;
-    wall clock. The creation alone is also reported."""
+    then copy the final node types, density and velocity into page-locked
+    host buffers (allocated before the timed region); wall clock. The
+    creation alone is also reported."""
     import torch
-    from lbm_solver_3d_b200.solver import Solver
+    from lbm_solver_3d_b200.solver import HostFields, Solver
+    out = HostFields(p.ncells, pinned=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = Solver(p)
@@ -443,9 +445,10 @@ def e2e_record(p, args):
         s2.run(k)
         traj_bytes += s2.traj_rows().nbytes
         remaining -= k
-    flag, rho, u = s2.fields()
+    flag, rho, u = s2.fields_into(out)
     t_e2e = time.perf_counter() - t0
     s2.close()
+    out.close()
     h2d = p.ncells * 1 + 4 * (p.ncells if p.squirmer else 0)  # flags + boundary-link set-up
     d2h = traj_bytes + flag.nbytes + rho.nbytes + u.nbytes
     world = dist_env()[0]
@@ -538,6 +541,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
                     help="measure the headline line only (no forms/accuracy/ensemble sub-records)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: warm-up and K steps of the workload, then each kernel timed alone; "
+                         "a short JSON line, no span, e2e or CPU legs (for a launch list or one ncu capture)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.precision_set = args.precision is not None
@@ -558,6 +564,20 @@ def main():
     world, rank, local = dist_env()
     import torch
     torch.cuda.set_device(local)
+    if args.profile:
+        from lbm_solver_3d_b200.solver import Solver
+        sol = Solver(p.update(device=local))
+        sol.run(args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol.run(args.steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        kt = sol.time_kernels(reps=4)
+        sol.close()
+        print(json.dumps({"profile": args.workload, "precision": args.precision, "steps": args.steps,
+                          "wall_ms_per_step": 1e3 * wall / args.steps, "kernels_ms": kt}), flush=True)
+        return
     pg = None
     if world > 1:
         import torch.distributed as dist

@@ -221,6 +221,15 @@ int lbmgpu_launch_count(const lbmgpu_handle* h, long long* n);
  * afterwards: use it on a handle kept for measurement. */
 int lbmgpu_time_kernels(lbmgpu_handle* h, int reps, double ms[3]);
 
+/* Failure detection without a fault: runs the bounded wait the device kernels
+ * use on an mbarrier that nothing arrives at, giving up after `limit` tries
+ * (1 .. 2^22; the kernels themselves use 2^22). *status receives the device
+ * status bits (16 = the watchdog gave up); the call returns
+ * LBMGPU_ERR_WATCHDOG in that case, as lbmgpu_run and lbmgpu_batch_run do
+ * when a wait of theirs gives up, and the device stays usable. No
+ * counterpart in the reference (its CPU loop has no waits to bound). */
+int lbmgpu_watchdog_selftest(int device, long long limit, int* status);
+
 /* Message of the last failure on this handle (or of lbmgpu_create on the
  * calling thread when h is NULL). Never NULL. */
 const char* lbmgpu_last_error(const lbmgpu_handle* h);

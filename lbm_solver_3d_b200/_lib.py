@@ -93,6 +93,7 @@ SIGNATURES = {
     "lbmgpu_mlp_forward": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float)]),
     "lbmgpu_mlp_forward_ex": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I, ctypes.POINTER(ctypes.c_float), _I]),
     "lbmgpu_mlp_last_error": (ctypes.c_char_p, [_P]),
+    "lbmgpu_watchdog_selftest": (_I, [_I, ctypes.c_longlong, ctypes.POINTER(_I)]),
     "lbmgpu_snapshot_begin": (_I, [_P]),
     "lbmgpu_snapshot_read": (_I, [_P, _U8P, _DP, _DP]),
     "lbmgpu_snapshot_last_error": (ctypes.c_char_p, [_P]),

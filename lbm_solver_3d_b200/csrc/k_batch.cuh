@@ -360,11 +360,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* m, unsigned bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* m) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
 }
-// true once the phase with the given parity has completed; false after the
-// iteration limit (each try_wait also suspends for a while in hardware)
-__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
+// true once the phase with the given parity has completed; false after
+// `limit` tries (each try_wait also suspends for a while in hardware)
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* m, uint32_t parity, long long limit) {
     const uint32_t a = smem_u32(m);
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -375,6 +375,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
     }
     return false;
 }
+constexpr long long MBAR_WAIT_LIMIT = 1ll << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) { return mbar_wait_n(m, parity, MBAR_WAIT_LIMIT); }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* m) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m))

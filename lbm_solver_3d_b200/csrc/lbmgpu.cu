@@ -35,6 +35,7 @@
 
 #include "../../include/lbmgpu.h"
 #include "k_aux.cuh"
+#include "k_batch.cuh"
 #include "k_squirmer.cuh"
 #include "launch.h"
 
@@ -106,7 +107,9 @@ struct lbmgpu_handle {
     long long traj_read = 0;
     long long launches = 0;
     bool pending_corr = false;   // a correction computed by the last step is still to be applied
-    Graph g;
+    // captured step patterns; index 1: the first step applies the mass
+    // correction computed by the step before the pattern
+    Graph g[2];
     std::string err;
     // ensemble member: populations and flags live in the ensemble's pools,
     // work is issued by the ensemble on its streams
@@ -445,9 +448,11 @@ int validate_impl(const lbmgpu_params* p, std::string& m) {
 }
 
 void drop_graph(lbmgpu_handle* h) {
-    if (h->g.exec) cudaGraphExecDestroy(h->g.exec);
-    if (h->g.graph) cudaGraphDestroy(h->g.graph);
-    h->g = Graph{};
+    for (Graph& g : h->g) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        g = Graph{};
+    }
 }
 
 void free_all(lbmgpu_handle* h) {
@@ -520,26 +525,34 @@ void fused_end(lbmgpu_handle* h, cudaStream_t sa, cudaStream_t sb) {
     cudaStreamWaitEvent(sa, h->ev_join, 0);
 }
 
-int ensure_graph(lbmgpu_handle* h, int steps) {
-    if (h->g.exec && h->g.steps == steps) return LBMGPU_OK;
-    drop_graph(h);
+// The captured pattern of `steps` steps. It starts at a step s with
+// (s - 1) % period == 0; apply0 says whether its first step applies a
+// correction computed by the step before (the usual case once the run is
+// under way: the period is a multiple of the correction interval, so the
+// step before a pattern is a correction step). Without corrections in the
+// pattern, the graph is only launched over stretches that contain no
+// correction step.
+int ensure_graph(lbmgpu_handle* h, int steps, bool apply0) {
+    Graph& g = h->g[apply0 ? 1 : 0];
+    if (g.exec && g.steps == steps) return LBMGPU_OK;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = Graph{};
     CUDA_TRY(h, cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
     const long long saved = h->launches;
     fused_begin(h, h->cap, h->cap2);
-    // the pattern starts at a step s with (s - 1) % period == 0
-    // (without corrections in the pattern, the graph is only launched over
-    // stretches that contain no correction step)
     for (int k = 0; k < steps; ++k) {
         const long long s = 1 + k;
-        StepPlan sp = plan_step(h, s, false, h->corr_in_graph && k > 0 && is_corr_step(h, s - 1));
+        const bool apply = k == 0 ? apply0 : h->corr_in_graph && is_corr_step(h, s - 1);
+        StepPlan sp = plan_step(h, s, false, apply);
         if (!h->corr_in_graph) sp.corr = false;
         issue_fused(h, h->cap, h->cap2, sp);
     }
     fused_end(h, h->cap, h->cap2);
     h->launches = saved;
-    CUDA_TRY(h, cudaStreamEndCapture(h->cap, &h->g.graph));
-    CUDA_TRY(h, cudaGraphInstantiate(&h->g.exec, h->g.graph, 0));
-    h->g.steps = steps;
+    CUDA_TRY(h, cudaStreamEndCapture(h->cap, &g.graph));
+    CUDA_TRY(h, cudaGraphInstantiate(&g.exec, g.graph, 0));
+    g.steps = steps;
     return LBMGPU_OK;
 }
 
@@ -574,6 +587,7 @@ int check_status(lbmgpu_handle* h) {
         return fail(h, LBMGPU_ERR_DEVICE, "squirmer moved one lattice cell or more in a single step");
     if (st & ST_LINK_OVERFLOW) return fail(h, LBMGPU_ERR_DEVICE, "boundary-link list capacity exceeded");
     if (st & ST_REMAP_OVERFLOW) return fail(h, LBMGPU_ERR_DEVICE, "remap changed-node list capacity exceeded");
+    if (st & ST_WATCHDOG) return fail(h, LBMGPU_ERR_WATCHDOG, "a bounded device wait gave up");
     return LBMGPU_OK;
 }
 
@@ -838,7 +852,7 @@ int lbmgpu_run(lbmgpu_handle* h, int nsteps) {
         // A captured graph starts at a pattern boundary, ends before the last
         // step (which stores the macroscopic fields), and contains correction
         // steps only if the pattern period includes them.
-        bool graph_ok = !last && h->t_main % h->period == 0 && rem - 1 >= gsteps && !h->pending_corr;
+        bool graph_ok = !last && h->t_main % h->period == 0 && rem - 1 >= gsteps;
         if (graph_ok && h->has_sq && h->p.mass_correction_every > 0 && !h->corr_in_graph) {
             const int k = h->p.mass_correction_every;
             graph_ok = (h->t_main / k) == ((h->t_main + gsteps) / k);  // no correction step inside
@@ -846,9 +860,9 @@ int lbmgpu_run(lbmgpu_handle* h, int nsteps) {
         if (graph_ok) {
             // the graph carries its own fork and join on the caller's stream
             fused_end(h, sa, sb);
-            int rc = ensure_graph(h, gsteps);
+            int rc = ensure_graph(h, gsteps, h->pending_corr);
             if (rc) return rc;
-            CUDA_TRY(h, cudaGraphLaunch(h->g.exec, sa));
+            CUDA_TRY(h, cudaGraphLaunch(h->g[h->pending_corr ? 1 : 0].exec, sa));
             h->launches += (long long)gsteps * per_step;
             h->t_main += gsteps;
             rem -= gsteps;
@@ -1504,7 +1518,7 @@ struct lbmgpu_batch {
     std::vector<long long> row_prefix;   // nodes in the rows before row r (rows away from walls)
     long long cells = 0, t = 0, launches = 0;
     bool pending_corr = false;
-    Graph g;
+    Graph g[2];   // captured patterns; index 1: the first step applies a pending correction
     std::string err;
 };
 
@@ -1523,9 +1537,10 @@ int bfail(lbmgpu_batch* b, int code, const std::string& msg) {
                          std::string(#call) + ": " + cudaGetErrorString(e_));                      \
     } while (0)
 
+void batch_drop_graphs(lbmgpu_batch* b);
+
 void batch_free(lbmgpu_batch* b) {
-    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
-    if (b->g.graph) cudaGraphDestroy(b->g.graph);
+    batch_drop_graphs(b);
     for (lbmgpu_handle* h : b->m) {
         h->member = true;
         free_all(h);
@@ -1628,24 +1643,36 @@ void batch_end(lbmgpu_batch* b, cudaStream_t sa, cudaStream_t sb) {
     cudaStreamWaitEvent(sa, b->ev_join, 0);
 }
 
-int batch_graph(lbmgpu_batch* b, int steps) {
-    if (b->g.exec && b->g.steps == steps) return LBMGPU_OK;
-    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
-    if (b->g.graph) cudaGraphDestroy(b->g.graph);
-    b->g = Graph{};
+// The ensemble's captured pattern (see ensure_graph): apply0 = its first
+// step applies the correction of the step before the pattern.
+int batch_graph(lbmgpu_batch* b, int steps, bool apply0) {
+    Graph& g = b->g[apply0 ? 1 : 0];
+    if (g.exec && g.steps == steps) return LBMGPU_OK;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = Graph{};
     BTRY(b, cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
     const long long saved = b->launches;
     batch_begin(b, b->cap, b->cap2);
     for (int k = 0; k < steps; ++k) {
         const long long s = 1 + k;
-        issue_batch(b, b->cap, b->cap2, s, false, b->corr_in_graph && k > 0 && is_corr_batch(b, s - 1), true);
+        const bool apply = k == 0 ? apply0 : b->corr_in_graph && is_corr_batch(b, s - 1);
+        issue_batch(b, b->cap, b->cap2, s, false, apply, true);
     }
     batch_end(b, b->cap, b->cap2);
     b->launches = saved;
-    BTRY(b, cudaStreamEndCapture(b->cap, &b->g.graph));
-    BTRY(b, cudaGraphInstantiate(&b->g.exec, b->g.graph, 0));
-    b->g.steps = steps;
+    BTRY(b, cudaStreamEndCapture(b->cap, &g.graph));
+    BTRY(b, cudaGraphInstantiate(&g.exec, g.graph, 0));
+    g.steps = steps;
     return LBMGPU_OK;
+}
+
+void batch_drop_graphs(lbmgpu_batch* b) {
+    for (Graph& g : b->g) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        g = Graph{};
+    }
 }
 
 int batch_status(lbmgpu_batch* b) {
@@ -1894,16 +1921,16 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
     long long rem = nsteps;
     while (rem > 0) {
         const bool last = rem == 1;
-        bool graph_ok = !last && b->t % b->period == 0 && rem - 1 >= gsteps && !b->pending_corr;
+        bool graph_ok = !last && b->t % b->period == 0 && rem - 1 >= gsteps;
         if (graph_ok && b->has_sq && b->p0.mass_correction_every > 0 && !b->corr_in_graph) {
             const int k = b->p0.mass_correction_every;
             graph_ok = (b->t / k) == ((b->t + gsteps) / k);
         }
         if (graph_ok) {
             batch_end(b, sa, sb);
-            int rc = batch_graph(b, gsteps);
+            int rc = batch_graph(b, gsteps, b->pending_corr);
             if (rc) return rc;
-            BTRY(b, cudaGraphLaunch(b->g.exec, sa));
+            BTRY(b, cudaGraphLaunch(b->g[b->pending_corr ? 1 : 0].exec, sa));
             b->launches += (long long)gsteps * per_step;
             b->t += gsteps;
             rem -= gsteps;
@@ -1937,9 +1964,7 @@ int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (rc) return rc;
     b->tile = tile;
     b->bps = ctas_per_sm;
-    if (b->g.exec) cudaGraphExecDestroy(b->g.exec);
-    if (b->g.graph) cudaGraphDestroy(b->g.graph);
-    b->g = Graph{};
+    batch_drop_graphs(b);
     return LBMGPU_OK;
 }
 
@@ -2046,6 +2071,43 @@ const char* lbmgpu_batch_last_error(const lbmgpu_batch* b) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+//  lbmgpu_watchdog_selftest: the bounded-wait path of the device kernels,
+//  exercised without a fault. One CTA waits on a shared-memory mbarrier that
+//  nothing arrives at, with the given try limit; when the wait gives up the
+//  kernel sets ST_WATCHDOG in a status word and returns, as the staged bulk
+//  kernel does, and the host turns that into LBMGPU_ERR_WATCHDOG.
+// ============================================================================
+namespace {
+__global__ void k_watchdog_selftest(long long limit, int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *status = mbar_wait_n(&bar, 0u, limit) ? 0 : ST_WATCHDOG;
+}
+}  // namespace
+
+extern "C" int lbmgpu_watchdog_selftest(int device, long long limit, int* status) {
+    if (!status || limit < 1 || limit > MBAR_WAIT_LIMIT)
+        return fail(nullptr, LBMGPU_ERR_INVALID, "lbmgpu_watchdog_selftest: limit must be 1..2^22 tries");
+    int* d = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMalloc(&d, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        k_watchdog_selftest<<<1, 32>>>(limit, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return fail(nullptr, LBMGPU_ERR_CUDA, std::string("lbmgpu_watchdog_selftest: ") + cudaGetErrorString(e));
+    if (*status & ST_WATCHDOG) return fail(nullptr, LBMGPU_ERR_WATCHDOG, "a bounded device wait gave up");
+    return LBMGPU_OK;
+}
 
 // ============================================================================
 //  lbmgpu_field_stats_static: the diagnostics of lbmgpu_diag over fields in the

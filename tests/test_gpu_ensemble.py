@@ -144,3 +144,27 @@ def test_member_handles_are_read_only(api):
             m.set_f(m.get_f())
         ens.run(3)
         assert m.t == 3
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_config4_ensemble_members_equal_alone(api, precision):
+    """The 256-member slit-channel ensemble of the benchmark (Nx 64-160, Ny/Nz
+    48-96, a 4-8, beta -5..5, seed 2024; 153 M nodes) with the autotuned bulk
+    tiling: after 60 steps (a graph chunk and single steps, six mass
+    corrections), five seeded members -- the smallest, the largest and three
+    drawn at random -- equal the same lattices run alone, bit for bit."""
+    from lbm_solver_3d_b200.workloads import ensemble_members
+    Ensemble, Solver = api
+    ps = ensemble_members(256)
+    for p in ps:
+        p.update(precision=precision)
+    sizes = [p.ncells for p in ps]
+    pick = {int(np.argmin(sizes)), int(np.argmax(sizes))}
+    pick |= set(np.random.default_rng(11).choice(256, 3, replace=False).tolist())
+    with Ensemble(ps) as ens:
+        assert ens.cells == sum(sizes)
+        tune = ens.autotune(reps=2)
+        print(f"{precision}: tiling {tune}")
+        ens.run(60)
+        for i in sorted(pick):
+            assert_member_equals_alone(ens, i, ps[i], Solver, [60])
