@@ -364,6 +364,11 @@ int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
  *     (grid = chunks / 4, ctas_per_sm unused);
  *   tile = LBMGPU_TILE_CHUNKP: the same chunks walked by persistent warps
  *     (grid = ctas_per_sm x SMs, 4 warps per CTA);
+ *   tile = LBMGPU_TILE_RUNS: on steps without sums, runs of consecutive rows
+ *     of one member's z-plane (contiguous in memory) are copied into
+ *     shared memory by bulk asynchronous copies, several runs deep, while
+ *     eight warps per CTA update the runs already staged (grid = ctas_per_sm
+ *     x SMs, persistent); steps with sums use the persistent chunks;
  *   tile = LBMGPU_TILE_STAGED3 / _STAGED4: each CTA owns a contiguous range
  *     of rows (equal node counts); a producer warp stages every row's
  *     populations and flags in shared memory with bulk asynchronous copies,
@@ -372,6 +377,7 @@ int lbmgpu_batch_size(const lbmgpu_batch* b, int* members, long long* cells);
 #define LBMGPU_TILE_ROWCTA 1
 #define LBMGPU_TILE_CHUNK 2
 #define LBMGPU_TILE_CHUNKP 3
+#define LBMGPU_TILE_RUNS 4
 #define LBMGPU_TILE_STAGED3 (-3)
 #define LBMGPU_TILE_STAGED4 (-4)
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm);

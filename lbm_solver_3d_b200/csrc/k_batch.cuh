@@ -39,6 +39,14 @@ __device__ __forceinline__ void chunk_reduce(NodeSums& s) {
     }
 }
 
+// Resident 128-thread CTAs per SM the ensemble's row and chunk kernels are
+// compiled for: 7 (72 registers) with FP32 arithmetic, 4 (128) with FP64
+// arithmetic (the FP64 form and FP32 storage), which spills at 72.
+template <class S>
+__host__ __device__ constexpr int batch_min_blocks() {
+    return S::shifted && sizeof(typename S::A) == 4 ? 7 : 4;
+}
+
 template <class S, int PAR, bool MACRO, bool WR, int TX>
 __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args,
                                                     const RowRef* __restrict__ rows, int nrows,
@@ -114,7 +122,7 @@ __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ 
 constexpr int ROWCTA_THREADS = 128;
 
 template <class S, int PAR, bool MACRO, bool WR>
-__global__ void __launch_bounds__(ROWCTA_THREADS, S::shifted ? 7 : 4) k_bulk_rowcta(const Lattice* __restrict__ lat,
+__global__ void __launch_bounds__(ROWCTA_THREADS, batch_min_blocks<S>()) k_bulk_rowcta(const Lattice* __restrict__ lat,
                                                                 const StreamArgs* __restrict__ args,
                                                                 const RowRef* __restrict__ rows,
                                                                 double* __restrict__ row_part, BatchStep st) {
@@ -182,7 +190,7 @@ __global__ void __launch_bounds__(ROWCTA_THREADS, S::shifted ? 7 : 4) k_bulk_row
 constexpr int CHUNK_WARPS = 4;
 
 template <class S, int PAR, bool MACRO>
-__global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_chunk(
+__global__ void __launch_bounds__(32 * CHUNK_WARPS, batch_min_blocks<S>()) k_bulk_chunk(
     const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args, const ChunkRef* __restrict__ chunks,
     int nchunks, double* __restrict__ chunk_part, BatchStep st) {
     __shared__ __align__(16) Lattice sL[CHUNK_WARPS];
@@ -237,7 +245,7 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_c
 // at (x0, y) and continues into the next rows of the same z-plane, and no
 // partials are written.
 template <class S, int PAR, bool MACRO, bool FLAT = false>
-__global__ void __launch_bounds__(32 * CHUNK_WARPS, S::shifted ? 7 : 4) k_bulk_chunkp(
+__global__ void __launch_bounds__(32 * CHUNK_WARPS, batch_min_blocks<S>()) k_bulk_chunkp(
     const Lattice* __restrict__ lat, const StreamArgs* __restrict__ args, const ChunkRef* __restrict__ chunks,
     int nchunks, double* __restrict__ chunk_part, BatchStep st) {
     __shared__ __align__(16) Lattice sL[CHUNK_WARPS];
@@ -600,13 +608,357 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
     }
 }
 
+// ---------------------------------------------------------------------------
+//  k_bulk_runs<S, PAR>: the rows away from walls of every member on a step
+//  without sums, staged through shared memory in runs: a run is up to
+//  RunsCfg<S>::NODES nodes of consecutive interior rows of one member's z-plane,
+//  which are consecutive in memory for every direction (odd steps read the rows
+//  of the plane shifted by the direction's (c_y, c_z), again consecutive;
+//  walls in y keep y - c_y inside the plane, and a run that would wrap in y is
+//  a single row). One producer warp copies the 19 ranges and the flags of a
+//  run with bulk asynchronous copies (from the 16-byte boundary below each
+//  range, rounded up: never outside the member's padded slice) into one of NST
+//  stages; eight update warps update the run's nodes from the stage with
+//  update_node's arithmetic and release it. Persistent CTAs take runs
+//  blockIdx.x + k * gridDim.x. Bounded waits and the drain on exit as in
+//  k_bulk_staged. The populations do not depend on how rows are grouped, so
+//  members stay bit-identical to lattices run alone; steps with sums use the
+//  chunk kernels, which form the row partials in k_bulk's order.
+// ---------------------------------------------------------------------------
+constexpr int RUNS_UPDATE_WARPS = 8;
+constexpr int RUNS_THREADS = 32 * (1 + RUNS_UPDATE_WARPS);
+template <class S> struct RunsCfg;
+template <> struct RunsCfg<StoreF64> { static constexpr int NST = 2, NODES = 256; };
+template <> struct RunsCfg<StoreF32> { static constexpr int NST = 3, NODES = 384; };
+template <> struct RunsCfg<StoreF16> { static constexpr int NST = 4, NODES = 512; };
+static_assert(RunsCfg<StoreF64>::NODES >= BATCH_MAX_NX, "a run holds at least one row of every member");
+// elements per staged direction range (a run plus the 16-byte rounding at both
+// ends), flag bytes per stage, bytes per stage (all multiples of 16)
+template <class S> __host__ __device__ constexpr int runs_cap() {
+    return RunsCfg<S>::NODES + 32 / (int)sizeof(typename S::T);
+}
+template <class S> __host__ __device__ constexpr int runs_fcap() { return RunsCfg<S>::NODES + 32; }
+template <class S> __host__ __device__ constexpr size_t runs_stage_bytes() {
+    return (size_t)Q * runs_cap<S>() * sizeof(typename S::T) + runs_fcap<S>();
+}
+
+// populations of node (row, x) of a staged run
+template <class T>
+struct RunSrc {
+    const T* sb;
+    const int* off;     // element offset of each direction's range in its slot
+    int cap, x, nx, row;
+    template <class S, int PAR, class V>
+    __device__ __forceinline__ void load(const T*, unsigned, unsigned, const Nbr&, V* v) const {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            int xs = x;
+            if (PAR == 1) {
+                xs = x - CX(i);
+                if (xs < 0) xs += nx; else if (xs >= nx) xs -= nx;
+            }
+            v[i] = (V)S::ld(sb + i * cap + off[i] + row * nx + xs);
+        }
+    }
+};
+
+template <class S, int PAR>
+__global__ void __launch_bounds__(RUNS_THREADS, 2) k_bulk_runs(const Lattice* __restrict__ lat,
+                                                            const StreamArgs* __restrict__ args,
+                                                            const int4* __restrict__ runs, int nruns, BatchStep st) {
+    using T = typename S::T;
+    constexpr int NST = RunsCfg<S>::NST, MS = NST + 1, CAP = runs_cap<S>(), FCAP = runs_fcap<S>();
+    constexpr size_t STAGE = runs_stage_bytes<S>();
+    extern __shared__ __align__(128) unsigned char runs_raw[];
+    __shared__ __align__(8) uint64_t full[NST], empty[NST];
+    __shared__ __align__(16) Lattice recL[MS];
+    __shared__ __align__(16) StreamArgs recA[MS];
+    __shared__ ZoneBox recZ[MS];
+    __shared__ int sSlot[NST], sOff[NST][Q], sFoff[NST];
+    __shared__ int4 sRun[NST];
+    __shared__ volatile int s_abort;
+    __shared__ int s_issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int q = 0; q < NST; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], RUNS_UPDATE_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+        s_issued = 0;
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        int last_m = -1, slot = -1;
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nruns; ++k) {
+            const int q = k % NST;
+            if (k >= NST) {
+                int go = 1;
+                if (lane == 0) {
+                    const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
+                    if (!ok && !s_abort) { s_abort = 1; atomicOr(&args[0].sq->status, ST_WATCHDOG); }
+                    go = ok && !s_abort;
+                }
+                if (!__shfl_sync(0xffffffffu, go, 0)) break;
+            }
+            const int4 run = runs[blockIdx.x + k * gridDim.x];   // (m, y0, z, nrow)
+            if (run.x != last_m) {
+                slot = (slot + 1) % MS;
+                const uint32_t* srcl = reinterpret_cast<const uint32_t*>(lat + run.x);
+                uint32_t* dstl = reinterpret_cast<uint32_t*>(&recL[slot]);
+                for (int w = lane; w < (int)(sizeof(Lattice) / 4); w += 32) dstl[w] = srcl[w];
+                const uint32_t* srca = reinterpret_cast<const uint32_t*>(args + run.x);
+                uint32_t* dsta = reinterpret_cast<uint32_t*>(&recA[slot]);
+                for (int w = lane; w < (int)(sizeof(StreamArgs) / 4); w += 32) dsta[w] = srca[w];
+                if (lane == 0) recZ[slot] = args[run.x].sq->zone[st.zslot];
+                __syncwarp();
+                if (lane == 0) {
+                    recA[slot].zslot = st.zslot; recA[slot].do_mass = st.do_mass; recA[slot].apply_corr = st.apply_corr;
+                }
+                last_m = run.x;
+                __syncwarp();
+            }
+            const Lattice& L = recL[slot];
+            const size_t cnt = (size_t)run.w * L.nx;
+            unsigned char* sb = runs_raw + (size_t)q * STAGE;
+            uintptr_t start = 0;
+            unsigned len = 0;
+            int ob = 0;
+            if (lane < Q) {
+                const int i = lane;
+                int ys = run.y, zs = run.z, arr = i;
+                if (PAR == 1) {
+                    arr = c_opp_rt(i);
+                    ys = run.y - c_cy_rt(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
+                    zs = run.z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
+                }
+                const T* f = static_cast<const T*>(recA[slot].f);
+                span16(f + (size_t)arr * L.N + (size_t)L.nx * (ys + (size_t)L.ny * zs), cnt * sizeof(T), start, len, ob);
+                sOff[q][i] = ob / (int)sizeof(T);
+            } else if (lane == Q) {
+                span16(recA[slot].flag + (size_t)L.nx * (run.y + (size_t)L.ny * run.z), cnt, start, len, ob);
+                sFoff[q] = ob;
+            }
+            unsigned total = len;
+            for (int o = 16; o > 0; o >>= 1) total += __shfl_down_sync(0xffffffffu, total, o);
+            if (lane == 0) {
+                sSlot[q] = slot; sRun[q] = run;
+                mbar_expect_tx(&full[q], total);   // releases the records written above
+            }
+            __syncwarp();
+            if (lane < Q)
+                bulk_g2s(sb + (size_t)lane * CAP * sizeof(T), reinterpret_cast<const void*>(start), len, &full[q]);
+            else if (lane == Q)
+                bulk_g2s(sb + (size_t)Q * CAP * sizeof(T), reinterpret_cast<const void*>(start), len, &full[q]);
+            if (lane == 0) s_issued = k + 1;
+            __syncwarp();
+        }
+    } else {
+        // ---------------- update warps ----------------
+        const int ut = tid - 32;
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nruns; ++k) {
+            const int q = k % NST;
+            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&args[0].sq->status, ST_WATCHDOG); }
+                break;
+            }
+            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;
+            const int slot = sSlot[q];
+            const Lattice& L = recL[slot];
+            const StreamArgs& a = recA[slot];
+            const int4 run = sRun[q];
+            const T* sb = reinterpret_cast<const T*>(runs_raw + (size_t)q * STAGE);
+            const uint8_t* sf = runs_raw + (size_t)q * STAGE + (size_t)Q * CAP * sizeof(T) + sFoff[q];
+            const int cnt = run.w * L.nx;
+            const unsigned n0 = (unsigned)L.nx * ((unsigned)run.y + (unsigned)L.ny * (unsigned)run.z);
+            for (int j = ut; j < cnt; j += 32 * RUNS_UPDATE_WARPS) {
+                const int row = j / L.nx, x = j - row * L.nx, y = run.y + row;
+                const bool active = (sf[j] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, recZ[slot], x, y, run.z);
+                if (active) {
+                    NodeSums sums;
+                    update_node<S, PAR, false, false>(L, a, n0 + (unsigned)j, x, y, run.z, 0, 0, false, sums,
+                                                      RunSrc<T>{sb, sOff[q], CAP, x, L.nx, row});
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[q]);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_abort) {
+        const int issued = s_issued;
+        for (int q = 0; q < NST && q < issued; ++q) mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+//  k_bulk_rows<S, PAR, SQ>: the rows away from walls of a single lattice on a
+//  step without sums, staged through shared memory by the bulk-copy engine.
+//
+//  A bulk kernel that loads its populations into registers is bound by how
+//  many bytes each SM keeps in flight: 19 loads per thread in flight at the
+//  occupancy the registers allow (measured on the 256x128x128 lattice: ~117 KB
+//  per SM -> 0.90 of the copy rate, ~78 KB -> 0.80, ~39 KB -> 0.50). Here the
+//  loads do not occupy registers: each CTA keeps RowsCfg<S>::NST whole x-rows
+//  of all 19 directions (plus the row's flags) in flight in shared memory.
+//
+//  CTA = one producer warp + nx update threads (nx a multiple of 32, at most
+//  ROWS_MAX_NX), persistent over the interior rows r = blockIdx.x + k *
+//  gridDim.x (y = ylo + r % nry, z = zlo + r / nry).
+//    producer   per row: waits for the stage to be free (empty barrier), then
+//               lane i < 19 copies direction-row i of the state -- A[i] of row
+//               (y, z) on an even step, A[opp(i)] of row (y - c_iy, z - c_iz)
+//               on an odd step, always a whole row, 16-byte aligned -- and
+//               lane 19 the row's flags, completing on the full barrier;
+//    update     thread x waits for the row (full barrier), reads its 19
+//               logical populations from the stage (odd step: x - c_ix,
+//               wrapped, inside the staged row), updates the node with the
+//               same arithmetic as k_bulk and stores straight to global
+//               memory, then releases the stage.
+//  Every wait is bounded; on a timeout ST_WATCHDOG is set, all warps leave
+//  their loops, and after the CTA's last barrier one thread waits (bounded)
+//  for the last copy armed into each stage before the CTA exits.
+// ---------------------------------------------------------------------------
+constexpr int ROWS_MAX_NX = 256;
+template <class S> struct RowsCfg;
+template <> struct RowsCfg<StoreF64> { static constexpr int NST = 2, MINB = 2; };
+template <> struct RowsCfg<StoreF32> { static constexpr int NST = 4, MINB = 2; };
+template <> struct RowsCfg<StoreF16> { static constexpr int NST = 6, MINB = 3; };
+
+template <class S>
+__host__ __device__ constexpr size_t rows_stage_bytes(int nx) {
+    return (size_t)Q * nx * sizeof(typename S::T) + (size_t)nx;   // nx % 32 == 0: every part 16-byte aligned
+}
+
+// Populations of node x from a staged row (whole direction-rows of nx elements).
+template <class T>
+struct RowSrc {
+    const T* sb;
+    int nx, x;
+    template <class S, int PAR, class V>
+    __device__ __forceinline__ void load(const T*, unsigned, unsigned, const Nbr&, V* v) const {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            int xs = x;
+            if (PAR == 1) {
+                xs = x - CX(i);
+                if (xs < 0) xs += nx; else if (xs >= nx) xs -= nx;
+            }
+            v[i] = (V)S::ld(sb + i * nx + xs);
+        }
+    }
+};
+
+template <class S, int PAR, bool SQ>
+__global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_rows(const Lattice L, const StreamArgs a,
+                                                                                 int nry, int nrows, int ylo, int zlo) {
+    using T = typename S::T;
+    constexpr int NST = RowsCfg<S>::NST;
+    extern __shared__ __align__(128) unsigned char rows_raw[];
+    __shared__ __align__(8) uint64_t full[NST], empty[NST];
+    __shared__ ZoneBox zb;
+    __shared__ volatile int s_abort;
+    __shared__ int s_issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nx = L.nx, nupd = nx >> 5;
+    const size_t stage = rows_stage_bytes<S>(nx);
+    if (tid == 0) {
+        for (int q = 0; q < NST; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], nupd);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+        s_issued = 0;
+        if (SQ) zb = a.sq->zone[a.zslot];
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        const T* f = static_cast<const T*>(a.f);
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
+            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
+            if (k >= NST) {
+                int go = 1;
+                if (lane == 0) {
+                    const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
+                    if (!ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                    go = ok && !s_abort;
+                }
+                if (!__shfl_sync(0xffffffffu, go, 0)) break;
+            }
+            const int y = ylo + r % nry, z = zlo + r / nry;
+            unsigned char* sb = rows_raw + (size_t)q * stage;
+            if (lane == 0) mbar_expect_tx(&full[q], (unsigned)stage);
+            __syncwarp();
+            if (lane < Q) {
+                const int i = lane;
+                int ys = y, zs = z, arr = i;
+                if (PAR == 1) {
+                    arr = c_opp_rt(i);
+                    ys = y - c_cy_rt(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
+                    zs = z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
+                }
+                bulk_g2s(sb + (size_t)i * nx * sizeof(T), f + (size_t)arr * L.N + (size_t)nx * (ys + (size_t)L.ny * zs),
+                         (unsigned)(nx * sizeof(T)), &full[q]);
+            } else if (lane == Q) {
+                bulk_g2s(sb + (size_t)Q * nx * sizeof(T), a.flag + (size_t)nx * (y + (size_t)L.ny * z), (unsigned)nx,
+                         &full[q]);
+            }
+            if (lane == 0) s_issued = k + 1;
+            __syncwarp();
+        }
+    } else {
+        // ---------------- update threads ----------------
+        const int x = tid - 32;
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
+            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
+            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                break;
+            }
+            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;   // lane 0's view, so the warp leaves together
+            const int y = ylo + r % nry, z = zlo + r / nry;
+            const unsigned char* sb = rows_raw + (size_t)q * stage;
+            const uint8_t fl = sb[(size_t)Q * nx * sizeof(T) + x];
+            bool active = (fl & (uint8_t)~NEAR_WALL) == 0;
+            if (SQ && active) active = !in_zone(L, zb, x, y, z);
+            if (active) {
+                const unsigned n = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+                NodeSums sums;
+                update_node<S, PAR, false, false>(L, a, n, x, y, z, 0, 0, false, sums,
+                                                  RowSrc<T>{reinterpret_cast<const T*>(sb), nx, x});
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[q]);   // this warp is done with the stage
+        }
+    }
+    // after an abort, wait for the last copy armed into each stage (see k_bulk_staged)
+    __syncthreads();
+    if (tid == 0 && s_abort) {
+        const int issued = s_issued;
+        for (int q = 0; q < NST && q < issued; ++q) mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
+    }
+}
+
+// One CTA per zone block of every member: zblocks lists the (member, block)
+// pairs that exist (members' zones differ in size), so no CTA is launched for
+// a block beyond its member's zone.
 template <class S, int PAR, bool MACRO>
 __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone_batch(const Lattice* __restrict__ lat,
                                                                const StreamArgs* __restrict__ args,
+                                                               const int2* __restrict__ zblocks,
                                                                double* __restrict__ zone_part, int gzmax, BatchStep st) {
     __shared__ Lattice L;
     __shared__ StreamArgs A;
-    const int m = blockIdx.y;
+    const int2 mb = zblocks[blockIdx.x];
+    const int m = mb.x, blk = mb.y;
     if (threadIdx.x == 0) {
         L = lat[m];
         StreamArgs a = args[m];
@@ -614,16 +966,15 @@ __global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone_batch(const Lattice* __
         A = a;
     }
     __syncthreads();
-    if ((int)(blockIdx.x * BOUNDARY_BLOCK) >= A.zone_cells) return;  // block-uniform
     __shared__ __align__(16) SqState zsq;
     __shared__ LinkStash<S> stash[Q * BOUNDARY_BLOCK];
     copy_sq_state(&zsq, A.sq);
     __syncthreads();
     NodeSums sums;
-    zone_cell<S, PAR, true, MACRO>(L, A, blockIdx.x * BOUNDARY_BLOCK + threadIdx.x, sums, &zsq, stash);
+    zone_cell<S, PAR, true, MACRO>(L, A, blk * BOUNDARY_BLOCK + threadIdx.x, sums, &zsq, stash);
     if (MACRO || st.do_mass)
         block_reduce4<BOUNDARY_BLOCK>(sums.fw[0], sums.fw[1], sums.fw[2], sums.mass,
-                                      zone_part + ((size_t)m * gzmax + blockIdx.x) * BLOCK_PART);
+                                      zone_part + ((size_t)m * gzmax + blk) * BLOCK_PART);
 }
 
 }  // namespace lbmgpu

@@ -156,7 +156,7 @@ struct NodeSums {
 // Post-collision values of a zone block's particle links, [direction][thread]:
 // the population itself (FP64) or its deviation (shifted forms).
 template <class S>
-using LinkStash = typename std::conditional<S::shifted, float, double>::type;
+using LinkStash = typename S::A;
 
 // ---------------------------------------------------------------------------
 //  update_node: the whole LBM::step body for one fluid node n.
@@ -199,74 +199,101 @@ struct GlobalSrc {
     }
 };
 
+// Constants of the collision in the arithmetic A of a storage form (A = float:
+// the FP32 copies kept in Lattice; A = double: the FP64 values themselves).
+template <class A> struct Coll;
+template <> struct Coll<float> {
+    __device__ static float omP(const Lattice& L) { return L.omPf; }
+    __device__ static float omM(const Lattice& L) { return L.omMf; }
+    __device__ static float gP(const Lattice& L) { return L.gPf; }
+    __device__ static float F(const Lattice& L, int d) { return L.Ff[d]; }
+    __device__ static float cF(const Lattice& L, int i) { return L.cF[i]; }
+    __device__ static float cm(const Lattice& L, int i) { return L.cm[i]; }
+    __host__ __device__ static constexpr float w(int i) { return WF(i); }
+};
+template <> struct Coll<double> {
+    __device__ static double omP(const Lattice& L) { return L.omP; }
+    __device__ static double omM(const Lattice& L) { return L.omM; }
+    __device__ static double gP(const Lattice& L) { return L.gP; }
+    __device__ static double F(const Lattice& L, int d) { return L.F[d]; }
+    __device__ static double cF(const Lattice& L, int i) { return CX(i) * L.F[0] + CY(i) * L.F[1] + CZ(i) * L.F[2]; }
+    __device__ static double cm(const Lattice& L, int i) { return L.gM * 3.0 * WD(i) * cF(L, i); }
+    __host__ __device__ static constexpr double w(int i) { return WD(i); }
+};
+
 // Moments of a node in the shifted forms, from its 19 stored numbers d (storage
-// units: the deviation times S::SC): dr = sum of d, rho, and the Guo
-// half-force velocity (lbm.cpp:143-152).
-template <class S>
-__device__ __forceinline__ void shifted_moments(const Lattice& L, const float* d, float& dr, float& rho, float& u,
-                                                float& v, float& wz) {
-    float jx = 0.f, jy = 0.f, jz = 0.f;
-    dr = 0.f;
+// units: the deviation times S::SC), in the form's arithmetic A: dr = sum of d,
+// rho, and the Guo half-force velocity (lbm.cpp:143-152).
+template <class S, class A = typename S::A>
+__device__ __forceinline__ void shifted_moments(const Lattice& L, const float* d, A& dr, A& rho, A& u, A& v, A& wz) {
+    A jx = 0, jy = 0, jz = 0;
+    dr = 0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-        dr += d[i];
-        if (CX(i) > 0) jx += d[i]; else if (CX(i) < 0) jx -= d[i];
-        if (CY(i) > 0) jy += d[i]; else if (CY(i) < 0) jy -= d[i];
-        if (CZ(i) > 0) jz += d[i]; else if (CZ(i) < 0) jz -= d[i];
+        const A di = (A)d[i];
+        dr += di;
+        if (CX(i) > 0) jx += di; else if (CX(i) < 0) jx -= di;
+        if (CY(i) > 0) jy += di; else if (CY(i) < 0) jy -= di;
+        if (CZ(i) > 0) jz += di; else if (CZ(i) < 0) jz -= di;
     }
-    rho = 1.0f + dr * S::INV;
-    const float inv = 1.0f / rho;
-    u = (jx * S::INV + 0.5f * L.Ff[0]) * inv;
-    v = (jy * S::INV + 0.5f * L.Ff[1]) * inv;
-    wz = (jz * S::INV + 0.5f * L.Ff[2]) * inv;
+    rho = A(1) + dr * (A)S::INV;
+    const A inv = A(1) / rho;
+    u = (jx * (A)S::INV + A(0.5) * Coll<A>::F(L, 0)) * inv;
+    v = (jy * (A)S::INV + A(0.5) * Coll<A>::F(L, 1)) * inv;
+    wz = (jz * (A)S::INV + A(0.5) * Coll<A>::F(L, 2)) * inv;
 }
 
 // TRT + Guo post-collision values in storage units (lbm.cpp:162-172, deviation
-// form): the rest population, and one opposite pair (i, i+1) with f+, feq+ and
-// S+ shared and the odd parts of opposite signs. srho = S::SC * rho, k15 =
-// 1.5 |u|^2, uF = u . F. FORCE = false drops the Guo source terms, which
-// vanish for F = 0.
-template <class S, bool FORCE>
-__device__ __forceinline__ float rest_post(const Lattice& L, float d0, float dr, float srho, float k15, float uF) {
-    const float eP = WF(0) * (dr - srho * k15);
-    return FORCE ? d0 - L.omPf * (d0 - eP) - S::SC * L.gPf * WF(0) * 3.0f * uF : d0 - L.omPf * (d0 - eP);
+// form), in the form's arithmetic A: the rest population, and one opposite pair
+// (i, i+1) with f+, feq+ and S+ shared and the odd parts of opposite signs.
+// srho = S::SC * rho, k15 = 1.5 |u|^2, uF = u . F. FORCE = false drops the Guo
+// source terms, which vanish for F = 0.
+template <class S, bool FORCE, class A = typename S::A>
+__device__ __forceinline__ A rest_post(const Lattice& L, A d0, A dr, A srho, A k15, A uF) {
+    using C = Coll<A>;
+    const A eP = C::w(0) * (dr - srho * k15);
+    return FORCE ? d0 - C::omP(L) * (d0 - eP) - (A)S::SC * C::gP(L) * C::w(0) * A(3) * uF
+                 : d0 - C::omP(L) * (d0 - eP);
 }
-template <class S, bool FORCE>
-__device__ __forceinline__ void pair_post(const Lattice& L, int i, float di, float dio, float u, float v, float wz,
-                                          float dr, float srho, float k15, float uF, float& oi, float& oo) {
-    const float cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
-    const float w = WF(i);
-    const float eP = w * (dr + srho * (4.5f * cu * cu - k15));  // feq+ - w, storage units
-    const float eM = 3.0f * w * srho * cu;                       // feq-
-    const float fP = 0.5f * (di + dio), fM = 0.5f * (di - dio);
-    float A, B;
+template <class S, bool FORCE, class A = typename S::A>
+__device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, A u, A v, A wz, A dr, A srho, A k15,
+                                          A uF, A& oi, A& oo) {
+    using C = Coll<A>;
+    const A cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
+    const A w = C::w(i);
+    const A eP = w * (dr + srho * (A(4.5) * cu * cu - k15));  // feq+ - w, storage units
+    const A eM = A(3) * w * srho * cu;                        // feq-
+    const A fP = A(0.5) * (di + dio), fM = A(0.5) * (di - dio);
+    A a, b;
     if (FORCE) {
-        A = S::SC * L.gPf * w * (9.0f * cu * L.cF[i] - 3.0f * uF) - L.omPf * (fP - eP);
-        B = S::SC * L.cm[i] - L.omMf * (fM - eM);
+        a = (A)S::SC * C::gP(L) * w * (A(9) * cu * C::cF(L, i) - A(3) * uF) - C::omP(L) * (fP - eP);
+        b = (A)S::SC * C::cm(L, i) - C::omM(L) * (fM - eM);
     } else {
-        A = -L.omPf * (fP - eP);
-        B = -L.omMf * (fM - eM);
+        a = -C::omP(L) * (fP - eP);
+        b = -C::omM(L) * (fM - eM);
     }
-    oi = di + A + B;
-    oo = dio + A - B;
+    oi = di + a + b;
+    oo = dio + a - b;
 }
 
-// Collide and push of a node with only fluid neighbours, FP32 arithmetic on
-// stored numbers: the rest population, then one opposite pair at a time.
-template <class S, int PAR, bool FORCE>
+// Collide and push of a node with only fluid neighbours, in the form's
+// arithmetic on its stored numbers: the rest population, then one opposite
+// pair at a time; each value is rounded to the storage type once, as stored.
+template <class S, int PAR, bool FORCE, class A = typename S::A>
 __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
-                                            const Nbr& nb, const float* d, float dr, float srho, float u, float v,
-                                            float wz, float uF, float k15, bool do_mass, NodeSums& out) {
+                                            const Nbr& nb, const float* d, A dr, A srho, A u, A v, A wz, A uF, A k15,
+                                            bool do_mass, NodeSums& out) {
     {   // rest population: c = 0
-        const float o0 = rest_post<S, FORCE>(L, d[0], dr, srho, k15, uF);
+        const float o0 = (float)rest_post<S, FORCE>(L, (A)d[0], dr, srho, k15, uF);
         S::st(f + n, o0);
         if (do_mass) out.mass += (double)S::rt(o0) * S::INV;
     }
 #pragma unroll
     for (int i = 1; i < Q; i += 2) {
         const int io = i + 1;
-        float oi, oo;
-        pair_post<S, FORCE>(L, i, d[i], d[io], u, v, wz, dr, srho, k15, uF, oi, oo);
+        A ai, ao;
+        pair_post<S, FORCE>(L, i, (A)d[i], (A)d[io], u, v, wz, dr, srho, k15, uF, ai, ao);
+        const float oi = (float)ai, oo = (float)ao;
         if (PAR == 0) {
             S::st(f + (size_t)io * N + n, oi);
             S::st(f + (size_t)i * N + n, oo);
@@ -462,7 +489,8 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
             out.fw[0] += dpx; out.fw[1] += dpy; out.fw[2] += dpz;   // only wall links reach here
         }
     } else {
-        // ------- FP32 arithmetic on stored deviations (storage units) --------
+        // ---- shifted forms: stored deviations (storage units), arithmetic S::A ----
+        using AR = typename S::A;
         float d[Q];
         src.template load<S, PAR>(f, N, n, nb, d);
         if (a.apply_corr) {
@@ -470,29 +498,29 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
 #pragma unroll
             for (int i = 0; i < Q; ++i) d[i] += (float)(WD(i) * corr * S::SC);
         }
-        float dr, rho, u, v, wz;
+        AR dr, rho, u, v, wz;
         shifted_moments<S>(L, d, dr, rho, u, v, wz);
         if (GENERAL) out.rho = (double)rho;
         if (store_rho) a.rho[n] = 1.0 + (double)dr * S::INV;
         if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-        const float usq = u * u + v * v + wz * wz;
-        const float uF = u * L.Ff[0] + v * L.Ff[1] + wz * L.Ff[2];
-        const float k15 = 1.5f * usq;
-        const float srho = S::SC * rho;
+        const AR usq = u * u + v * v + wz * wz;
+        const AR uF = u * Coll<AR>::F(L, 0) + v * Coll<AR>::F(L, 1) + wz * Coll<AR>::F(L, 2);
+        const AR k15 = AR(1.5) * usq;
+        const AR srho = (AR)S::SC * rho;
         if (!boundary) {
             if (L.force_free)   // uniform: the Guo source terms are exactly zero
                 plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
             else
                 plain_pairs<S, PAR, true>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
         } else {
-            float post[Q];
-            post[0] = rest_post<S, true>(L, d[0], dr, srho, k15, uF);
+            AR post[Q];
+            post[0] = rest_post<S, true>(L, (AR)d[0], dr, srho, k15, uF);
 #pragma unroll
             for (int i = 1; i < Q; i += 2)
-                pair_post<S, true>(L, i, d[i], d[i + 1], u, v, wz, dr, srho, k15, uF, post[i], post[i + 1]);
+                pair_post<S, true>(L, i, (AR)d[i], (AR)d[i + 1], u, v, wz, dr, srho, k15, uF, post[i], post[i + 1]);
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
-                const float dpost = post[i];
+                const AR dpost = post[i];
                 const unsigned nbi = nb.of(n, i);
                 T* local = f + (size_t)OPP(i) * N + n;
                 T* remote = f + (size_t)i * N + nbi;
@@ -500,8 +528,9 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
                                    : GENERAL ? (uint8_t)((ntypes >> (2 * i)) & 3u)
                                              : (wall_dir(i, wallrow) ? T_WALL : T_FLUID);
                 if (tt == T_FLUID) {
-                    S::st(PAR == 0 ? local : remote, dpost);
-                    if (do_mass) out.mass += (double)S::rt(dpost) * S::INV;
+                    const float o = (float)dpost;
+                    S::st(PAR == 0 ? local : remote, o);
+                    if (do_mass) out.mass += (double)S::rt(o) * S::INV;
                     continue;
                 }
                 if (GENERAL && tt == T_PARTICLE) {   // finished by zone_particle_links
@@ -526,6 +555,15 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
     }
 }
 
+// Resident 256-thread CTAs per SM the bulk kernels are compiled for: FP32
+// arithmetic on stored deviations fits 64 registers (4); FP64 arithmetic on
+// FP32 storage spills at 80 and gets 128 (2); the FP64 form keeps 2 unless the
+// bulk is long (DENSE, see k_bulk).
+template <class S>
+__host__ __device__ constexpr int bulk_min_blocks(bool dense) {
+    return !S::shifted ? (dense ? 3 : 2) : (sizeof(typename S::A) == 8 ? 2 : 4);
+}
+
 // ---------------------------------------------------------------------------
 //  k_bulk<S, PAR, SQ, MACRO, WR>: fluid nodes without a PARTICLE neighbour,
 //  outside the zone.
@@ -543,7 +581,7 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
 //    DENSE (FP64 only) 3 CTAs/SM instead of 2 (80 registers, a few spills): for
 //          long bulks; a short one leaves room for the zone and squirmer chain
 template <class S, int PAR, bool SQ, bool MACRO, bool WR, bool DENSE = false>
-__global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk(const Lattice L, const StreamArgs a) {
+__global__ void __launch_bounds__(256, bulk_min_blocks<S>(DENSE)) k_bulk(const Lattice L, const StreamArgs a) {
     pdl_wait();
     pdl_launch_dependents();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -570,7 +608,7 @@ __global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk(
 // range of nodes; 256 threads take 256 consecutive nodes of it, so no lane
 // idles at a row's end. Grid (ceil(range / 256), planes away from z walls).
 template <class S, int PAR, bool SQ, bool DENSE = false>
-__global__ void __launch_bounds__(256, S::shifted ? 4 : (DENSE ? 3 : 2)) k_bulk_flat(const Lattice L, const StreamArgs a) {
+__global__ void __launch_bounds__(256, bulk_min_blocks<S>(DENSE)) k_bulk_flat(const Lattice L, const StreamArgs a) {
     pdl_wait();
     pdl_launch_dependents();
     const int ylo = L.walls_y ? 2 : 0, rows = L.walls_y ? L.ny - 4 : L.ny;
@@ -685,16 +723,20 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, co
             d0[i] += c; d1[i] += c;
         }
     }
-    float dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
+    using AR = typename S::A;
+    using C = Coll<AR>;
+    AR dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
     shifted_moments<S>(L, d0, dr0, rho0, u0, v0, w0);
     shifted_moments<S>(L, d1, dr1, rho1, u1, v1, w1);
-    const float k0 = 1.5f * (u0 * u0 + v0 * v0 + w0 * w0), k1 = 1.5f * (u1 * u1 + v1 * v1 + w1 * w1);
-    const float uF0 = u0 * L.Ff[0] + v0 * L.Ff[1] + w0 * L.Ff[2];
-    const float uF1 = u1 * L.Ff[0] + v1 * L.Ff[1] + w1 * L.Ff[2];
-    const float sr0 = S::SC * rho0, sr1 = S::SC * rho1;
+    const AR q0 = u0 * u0 + v0 * v0 + w0 * w0, q1 = u1 * u1 + v1 * v1 + w1 * w1;
+    const AR k0 = AR(1.5) * q0, k1 = AR(1.5) * q1;
+    const AR uF0 = u0 * C::F(L, 0) + v0 * C::F(L, 1) + w0 * C::F(L, 2);
+    const AR uF1 = u1 * C::F(L, 0) + v1 * C::F(L, 1) + w1 * C::F(L, 2);
+    const AR sr0 = (AR)S::SC * rho0, sr1 = (AR)S::SC * rho1;
 
     // ---- stores: post-collision value of direction i to its slot ----
-    // (a, b) = values of nodes x0, x0 + 1 for direction i
+    // (a0, a1) = the values of nodes x0, x0 + 1 for direction i, already
+    // rounded to the FP32 they are stored through
     auto put = [&](int i, float a0, float a1) {
         if (PAR == 0) {                                        // A[opp(i)][n]
             T* p = f + (size_t)OPP(i) * N + n0;
@@ -718,16 +760,17 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, co
             if (!has_prev && act0) S::st(rowp + xm, a0);
         }
     };
-    put(0, rest_post<S, FORCE>(L, d0[0], dr0, sr0, k0, uF0), rest_post<S, FORCE>(L, d1[0], dr1, sr1, k1, uF1));
+    put(0, (float)rest_post<S, FORCE>(L, (AR)d0[0], dr0, sr0, k0, uF0),
+        (float)rest_post<S, FORCE>(L, (AR)d1[0], dr1, sr1, k1, uF1));
 #pragma unroll
     for (int i = 1; i < Q; i += 2) {
-        float a0i, a0o, a1i, a1o;
-        pair_post<S, FORCE>(L, i, d0[i], d0[i + 1], u0, v0, w0, dr0, sr0, k0, uF0, a0i, a0o);
-        pair_post<S, FORCE>(L, i, d1[i], d1[i + 1], u1, v1, w1, dr1, sr1, k1, uF1, a1i, a1o);
+        AR a0i, a0o, a1i, a1o;
+        pair_post<S, FORCE>(L, i, (AR)d0[i], (AR)d0[i + 1], u0, v0, w0, dr0, sr0, k0, uF0, a0i, a0o);
+        pair_post<S, FORCE>(L, i, (AR)d1[i], (AR)d1[i + 1], u1, v1, w1, dr1, sr1, k1, uF1, a1i, a1o);
         // direction i's post value goes where the next state reads logical
         // f_i: even step -> A[opp(i)][n]; odd step -> A[i][n + c_i]
-        put(i, a0i, a1i);
-        put(i + 1, a0o, a1o);
+        put(i, (float)a0i, (float)a1i);
+        put(i + 1, (float)a0o, (float)a1o);
     }
 }
 

@@ -21,6 +21,10 @@ struct StreamGeom {
     bool dense;          // FP64: the bulk at 3 CTAs/SM (a long bulk)
     dim3 flat;           // k_bulk_flat's grid for steps without sums (x = 0: not used)
     dim3 pair, pair_block;   // k_bulk_pair's grid and block for steps without sums (x = 0: not used)
+    // k_bulk_rows (rows staged in shared memory) for steps without sums: grid
+    // (rows_grid = 0: not used), interior rows nry x (rows_n / nry) from (ylo, zlo)
+    unsigned rows_grid = 0;
+    int rows_nry = 0, rows_n = 0, rows_ylo = 0, rows_zlo = 0;
 };
 
 struct SqArgs;
@@ -34,13 +38,15 @@ struct BatchArgs {
     const RowRef* wrows; int nwrows;   // rows next to a wall
     double* row_part;                  // one entry per (member, y, z) row, both row kinds
     double* zone_part;
-    int gzmax;                         // zone blocks per member (grid x of the zone launch)
+    int gzmax;                         // zone-block entries per member in zone_part
+    const int2* zblocks; int nzblocks; // (member, block) of every zone block that exists
     int nmembers;
     const MemberParts* parts;
     const int* bounds;                 // staged kernel: row range of each CTA (grid + 1 entries)
     const ChunkRef* chunks; int nchunks;   // chunk kernel: 32-node pieces of the rows away from walls
     const RowChunks* rowchunks;        // chunk kernel: each row's chunks
     const ChunkRef* flat; int nflat;   // persistent chunk kernel, steps without sums: 32-node pieces of row runs
+    const int4* runs; int nruns;       // staged-run kernel: (member, y0, z, rows) of consecutive interior rows
     double* chunk_part;                // chunk kernel: partial sums per chunk
     int cap;                           // staged kernel: elements per staged direction-row
     int fcap;                          // staged kernel: bytes per staged flag row
@@ -74,6 +80,10 @@ struct Launchers {
     // one warp per 32-node chunk (k_bulk_chunk, then k_fold_chunks when summing)
     void (*batch_chunk)(int par, bool macro, bool sums, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
     int (*chunkp_ctas_per_sm)();   // resident CTAs per SM of the persistent chunk kernel
+    int (*rows_ctas_per_sm)(int nx);   // resident CTAs per SM of k_bulk_rows for rows of nx nodes
+    // rows away from walls in runs staged through shared memory (k_bulk_runs, steps without sums)
+    void (*batch_runs)(int par, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
+    int runs_max_nodes;                // nodes per run
     // one CTA per row (k_bulk_rowcta): rows away from walls, or next to one
     void (*batch_rowcta)(int par, bool macro, bool wallrows, const BatchArgs& b, BatchStep st, cudaStream_t s);
     size_t esize;

@@ -55,9 +55,18 @@ constexpr int ST_WATCHDOG = 16;      // a bounded wait for staged data gave up
 // as it is (for FP16 the scaled deviation), and SC / INV convert between
 // storage units and deviations (1 for FP32, so its arithmetic is unchanged).
 // T2 is the 2-element vector of the stored type (two x-adjacent nodes).
+// A is the arithmetic of the collision in each form. FP32 storage computes in
+// FP64: the moments of the stored numbers and the TRT update are then exact
+// enough that the collision conserves mass and momentum to FP64 rounding, and
+// the only FP32 rounding left is the store. (In FP32 arithmetic the moments'
+// rounding is re-injected into the flow every step; over the 10000 steps of the
+// 256x128x128 squirmer lattice that left u 1e-4 away from the FP64 form, against
+// 1e-8 with FP64 arithmetic.) FP16 storage keeps FP32 arithmetic: its storage
+// rounding (2^-11) dominates either way.
 struct StoreF64 {
     using T = double;
     using T2 = double2;
+    using A = double;
     static constexpr bool shifted = false;
     static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static double ld(const T* p) { return *p; }
@@ -67,6 +76,7 @@ struct StoreF64 {
 struct StoreF32 {
     using T = float;
     using T2 = float2;
+    using A = double;
     static constexpr bool shifted = true;
     static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static float ld(const T* p) { return *p; }
@@ -79,6 +89,7 @@ constexpr float FP16_SCALE = 4096.0f, FP16_INV_SCALE = 1.0f / 4096.0f;
 struct StoreF16 {
     using T = __half;
     using T2 = __half2;
+    using A = float;
     static constexpr bool shifted = true;
     static constexpr float SC = FP16_SCALE, INV = FP16_INV_SCALE;
     __device__ static float ld(const T* p) { return __half2float(*p); }
@@ -228,6 +239,9 @@ __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepc
 struct RowRef {
     int m, y, z;       // member, row coordinates
     int part;          // entry of the row's partial sums (member base + y + ny*z)
+};
+struct RunRef {        // nrow consecutive rows [y0, y0 + nrow) of one member's plane z: contiguous nodes
+    int m, y0, z, nrow;
 };
 struct ChunkRef {      // 32 consecutive nodes [x0, x0 + 32) of one row (the last may be short)
     int m, y, z, x0;

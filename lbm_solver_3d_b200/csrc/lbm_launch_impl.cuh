@@ -11,8 +11,16 @@
 
 namespace lbmgpu {
 
+template <class S>
+static size_t rows_smem(int nx) { return (size_t)RowsCfg<S>::NST * rows_stage_bytes<S>(nx); }
+
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
+    if (!MACRO && !a.do_mass && g.rows_grid) {   // no sums this step: rows staged in shared memory
+        k_bulk_rows<S, PAR, SQ><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(L, a, g.rows_nry, g.rows_n,
+                                                                                  g.rows_ylo, g.rows_zlo);
+        return;
+    }
     if constexpr (S::shifted && !MACRO) {
         if (!a.do_mass && g.pair.x) {   // no sums this step: two x-adjacent nodes per thread
             if (L.force_free) k_bulk_pair<S, PAR, SQ, false><<<g.pair, g.pair_block, 0, st>>>(L, a);
@@ -236,12 +244,13 @@ static cudaError_t staged_attr() {
 
 template <class S>
 static void batch_zone_launch(int par, bool macro, const BatchArgs& b, BatchStep st, cudaStream_t s) {
-    const dim3 grid(b.gzmax, b.nmembers);
+    if (b.nzblocks == 0) return;
+    const dim3 grid(b.nzblocks);
     switch ((par ? 2 : 0) | (macro ? 1 : 0)) {
-        case 0: k_zone_batch<S, 0, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
-        case 1: k_zone_batch<S, 0, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
-        case 2: k_zone_batch<S, 1, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
-        default: k_zone_batch<S, 1, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zone_part, b.gzmax, st); break;
+        case 0: k_zone_batch<S, 0, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zblocks, b.zone_part, b.gzmax, st); break;
+        case 1: k_zone_batch<S, 0, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zblocks, b.zone_part, b.gzmax, st); break;
+        case 2: k_zone_batch<S, 1, false><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zblocks, b.zone_part, b.gzmax, st); break;
+        default: k_zone_batch<S, 1, true><<<grid, BOUNDARY_BLOCK, 0, s>>>(b.lat, b.args, b.zblocks, b.zone_part, b.gzmax, st); break;
     }
 }
 
@@ -251,9 +260,36 @@ static void batch_squirmer_launch(const BatchArgs& b, SqStep st, cudaStream_t s)
 }
 
 template <class S>
+static void batch_runs_launch(int par, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s) {
+    if (b.nruns == 0) return;
+    const size_t smem = (size_t)RunsCfg<S>::NST * runs_stage_bytes<S>();
+    if (par) k_bulk_runs<S, 1><<<grid, RUNS_THREADS, smem, s>>>(b.lat, b.args, b.runs, b.nruns, st);
+    else k_bulk_runs<S, 0><<<grid, RUNS_THREADS, smem, s>>>(b.lat, b.args, b.runs, b.nruns, st);
+}
+
+template <class S>
+static int rows_occupancy(int nx) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows<S, 0, true>, 32 + nx, rows_smem<S>(nx)) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+template <class S>
 static cudaError_t prepare_launch() {
     cudaError_t e = cudaFuncSetAttribute(k_squirmer<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
     if (e != cudaSuccess) return e;
+    const int runs_smem = (int)((size_t)RunsCfg<S>::NST * runs_stage_bytes<S>());
+    for (auto fn : {k_bulk_runs<S, 0>, k_bulk_runs<S, 1>}) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, runs_smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int rs = (int)rows_smem<S>(ROWS_MAX_NX);
+    for (auto fn : {k_bulk_rows<S, 0, false>, k_bulk_rows<S, 0, true>, k_bulk_rows<S, 1, false>, k_bulk_rows<S, 1, true>}) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, rs);
+        if (e != cudaSuccess) return e;
+    }
     e = cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
     if (e != cudaSuccess) return e;
     cudaError_t es[8] = {staged_attr<S, 0, false, 3>(), staged_attr<S, 0, false, 4>(), staged_attr<S, 0, true, 3>(),
@@ -283,6 +319,9 @@ static Launchers make_launchers() {
     l.batch_rowcta = &batch_rowcta_launch<S>;
     l.batch_chunk = &batch_chunk_launch<S>;
     l.chunkp_ctas_per_sm = &chunkp_occupancy<S>;
+    l.rows_ctas_per_sm = &rows_occupancy<S>;
+    l.batch_runs = &batch_runs_launch<S>;
+    l.runs_max_nodes = RunsCfg<S>::NODES;
     l.esize = sizeof(typename S::T);
     return l;
 }

@@ -153,11 +153,15 @@ const Launchers* launchers_for(int prec) {
 
 size_t esize_for(int prec) { return prec == LBMGPU_FP64 ? 8 : (prec == LBMGPU_FP32 ? 4 : 2); }
 
-// LBMGPU_PAIR_BULK=0 in the environment keeps the one-node bulk kernel on
-// every step (for comparing the two; results are the same bit for bit).
-bool pair_bulk_disabled() {
-    const char* e = std::getenv("LBMGPU_PAIR_BULK");
-    return e && e[0] == '0';
+// The bulk kernel of steps without sums, where the lattice allows a choice:
+// LBMGPU_BULK=rows (rows staged in shared memory, the default), pair (two
+// nodes per thread, shifted forms) or node (one node per thread). The results
+// are the same bit for bit; the variable exists to compare their speed.
+int bulk_kind() {
+    const char* e = std::getenv("LBMGPU_BULK");
+    if (!e || !*e || !std::strcmp(e, "rows")) return 2;
+    if (!std::strcmp(e, "pair")) return 1;
+    return 0;
 }
 
 // Capacity of the boundary-link list of a lattice with these parameters (the
@@ -720,13 +724,27 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
         // updates two x-adjacent nodes per thread (k_bulk_pair); the block is
         // the largest multiple of 32 up to 128 threads that divides nx / 2
         h->geom.pair = dim3(0, 0, 0);
-        if (p->precision != LBMGPU_FP64 && p->nx % 64 == 0 && !pair_bulk_disabled()) {
+        if (p->precision != LBMGPU_FP64 && p->nx % 64 == 0 && bulk_kind() == 1) {
             const int pairs = p->nx / 2;
             int tb = 32;
             for (int b = 128; b >= 32; b -= 32)
                 if (pairs % b == 0) { tb = b; break; }
             h->geom.pair_block = dim3((unsigned)tb, 1, 1);
             h->geom.pair = dim3((unsigned)(pairs / tb), (unsigned)p->ny, (unsigned)p->nz);
+        }
+        // nx a multiple of 32 up to 256: rows staged in shared memory
+        // (k_bulk_rows), a persistent grid of the CTAs that fit on the SMs
+        h->geom.rows_grid = 0;
+        if (p->nx % 32 == 0 && p->nx <= ROWS_MAX_NX && rows > 0 && planes > 0 && bulk_kind() == 2) {
+            int sms = 0, dev = p->device;
+            const int per_sm = h->lz->rows_ctas_per_sm(p->nx);
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && per_sm > 0) {
+                h->geom.rows_nry = rows;
+                h->geom.rows_n = rows * planes;
+                h->geom.rows_ylo = p->walls_y ? 2 : 0;
+                h->geom.rows_zlo = p->walls_z ? 2 : 0;
+                h->geom.rows_grid = (unsigned)std::min<long long>((long long)sms * per_sm, (long long)rows * planes);
+            }
         }
     }
     h->link_cap = link_capacity(*p);
@@ -1502,6 +1520,8 @@ struct lbmgpu_batch {
     RowRef* d_rows = nullptr;
     RowRef* d_wrows = nullptr;
     MemberParts* d_parts = nullptr;
+    int2* d_zblocks = nullptr;     // (member, block) of every zone block
+    int4* d_runs = nullptr;        // staged-run kernel: runs of interior rows
     double *row_part = nullptr, *zone_part = nullptr;
     int* d_status = nullptr;
     BatchArgs ba{};
@@ -1547,7 +1567,7 @@ void batch_free(lbmgpu_batch* b) {
         delete h;
     }
     b->m.clear();
-    void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts,
+    void* ptrs[] = {b->fpool, b->flagpool, b->d_lat, b->d_args, b->d_sqargs, b->d_rows, b->d_wrows, b->d_parts, b->d_zblocks, b->d_runs,
                     b->row_part, b->zone_part, b->d_status, b->d_bounds, b->d_chunks, b->d_rowchunks,
                     b->chunk_part, b->d_flat};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -1595,6 +1615,12 @@ void launch_bulk(lbmgpu_batch* b, int tile, int grid, int par, bool macro, Batch
     else if (tile == LBMGPU_TILE_ROWCTA) b->lz->batch_rowcta(par, macro, false, b->ba, bst, s);
     else if (tile == LBMGPU_TILE_CHUNK) b->lz->batch_chunk(par, macro, macro || bst.do_mass, 0, b->ba, bst, s);
     else if (tile == LBMGPU_TILE_CHUNKP) b->lz->batch_chunk(par, macro, macro || bst.do_mass, grid, b->ba, bst, s);
+    else if (tile == LBMGPU_TILE_RUNS) {
+        if (macro || bst.do_mass)   // sums in k_bulk's row order: the persistent chunks, one wave
+            b->lz->batch_chunk(par, macro, true, b->sms * std::min(16, b->lz->chunkp_ctas_per_sm()), b->ba, bst, s);
+        else
+            b->lz->batch_runs(par, grid, b->ba, bst, s);
+    }
     else b->lz->batch_bulk(par, macro, false, tile, grid, b->ba, bst, s);
 }
 
@@ -1785,11 +1811,43 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
         parts[i].nzb = b->has_sq ? (int)b->m[i]->geom.bgrid : 0;
         gzmax = std::max(gzmax, parts[i].nzb);
     }
+    // runs of consecutive interior rows of a plane for the staged-run kernel:
+    // rows 0 and ny-1 (interior only without walls in y) stay single, so an
+    // odd step's source rows y - c_y of a longer run never wrap
+    std::vector<int4> runs;
+    {
+        const int maxn = b->lz->runs_max_nodes;
+        for (int i = 0; i < n; ++i) {
+            const lbmgpu_params& q = ps[i];
+            const int R = std::max(1, maxn / q.nx);
+            for (int z = 0; z < q.nz; ++z) {
+                int y = 0;
+                while (y < q.ny) {
+                    if (is_wall(q, y, z) || near_wall(q, y, z)) { ++y; continue; }
+                    int len = 1;
+                    if (y > 0 && y < q.ny - 1)
+                        while (len < R && y + len < q.ny - 1 && !is_wall(q, y + len, z) && !near_wall(q, y + len, z))
+                            ++len;
+                    runs.push_back(make_int4(i, y, z, len));
+                    y += len;
+                }
+            }
+        }
+    }
+    CB(cudaMalloc(&b->d_runs, std::max<size_t>(1, runs.size()) * sizeof(int4)));
+    if (!runs.empty())
+        CB(cudaMemcpy(b->d_runs, runs.data(), runs.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CB(cudaMalloc(&b->d_rows, std::max<size_t>(1, rows.size()) * sizeof(RowRef)));
     CB(cudaMalloc(&b->d_wrows, std::max<size_t>(1, wrows.size()) * sizeof(RowRef)));
     CB(cudaMalloc(&b->row_part, nparts * BLOCK_PART * sizeof(double)));
     CB(cudaMalloc(&b->zone_part, (size_t)n * gzmax * BLOCK_PART * sizeof(double)));
     CB(cudaMalloc(&b->d_parts, (size_t)n * sizeof(MemberParts)));
+    std::vector<int2> zblocks;
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < parts[i].nzb; ++k) zblocks.push_back(make_int2(i, k));
+    CB(cudaMalloc(&b->d_zblocks, std::max<size_t>(1, zblocks.size()) * sizeof(int2)));
+    if (!zblocks.empty())
+        CB(cudaMemcpy(b->d_zblocks, zblocks.data(), zblocks.size() * sizeof(int2), cudaMemcpyHostToDevice));
     CB(cudaMalloc(&b->d_lat, (size_t)n * sizeof(Lattice)));
     CB(cudaMalloc(&b->d_args, (size_t)n * sizeof(StreamArgs)));
     CB(cudaMalloc(&b->d_sqargs, (size_t)n * sizeof(SqArgs)));
@@ -1866,6 +1924,8 @@ int lbmgpu_batch_create(const lbmgpu_params* ps, int n, lbmgpu_batch** out) {
     b->ba.wrows = b->d_wrows; b->ba.nwrows = (int)wrows.size();
     b->ba.row_part = b->row_part; b->ba.zone_part = b->zone_part;
     b->ba.gzmax = gzmax; b->ba.nmembers = n; b->ba.parts = b->d_parts;
+    b->ba.zblocks = b->d_zblocks; b->ba.nzblocks = (int)zblocks.size();
+    b->ba.runs = b->d_runs; b->ba.nruns = (int)runs.size();
     {
         int nxmax = 1;
         for (int i = 0; i < n; ++i) nxmax = std::max(nxmax, ps[i].nx);
@@ -1952,10 +2012,11 @@ int lbmgpu_batch_run(lbmgpu_batch* b, int nsteps) {
 int lbmgpu_batch_set_tiling(lbmgpu_batch* b, int tile, int ctas_per_sm) {
     if (!b) return LBMGPU_ERR_INVALID;
     if ((tile != 32 && tile != 64 && tile != 128 && tile != LBMGPU_TILE_STAGED3 && tile != LBMGPU_TILE_STAGED4 &&
-         tile != LBMGPU_TILE_ROWCTA && tile != LBMGPU_TILE_CHUNK && tile != LBMGPU_TILE_CHUNKP) ||
+         tile != LBMGPU_TILE_ROWCTA && tile != LBMGPU_TILE_CHUNK && tile != LBMGPU_TILE_CHUNKP &&
+         tile != LBMGPU_TILE_RUNS) ||
         ctas_per_sm < 1 || ctas_per_sm > 16)
         return bfail(b, LBMGPU_ERR_INVALID, "tile must be 32, 64, 128 (threads per row), LBMGPU_TILE_ROWCTA, "
-                                            "LBMGPU_TILE_CHUNK or "
+                                            "LBMGPU_TILE_CHUNK(P), LBMGPU_TILE_RUNS or "
                                             "LBMGPU_TILE_STAGED3/4, and ctas_per_sm 1..16");
     BTRY(b, cudaSetDevice(b->p0.device));
     BTRY(b, cudaStreamSynchronize(b->sa));
@@ -1983,8 +2044,8 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     cudaEvent_t e0, e1;
     BTRY(b, cudaEventCreate(&e0));
     BTRY(b, cudaEventCreate(&e1));
-    const int tiles[8] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_CHUNKP, LBMGPU_TILE_ROWCTA, 32, 64, 128,
-                          LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4};
+    const int tiles[9] = {LBMGPU_TILE_CHUNK, LBMGPU_TILE_CHUNKP, LBMGPU_TILE_ROWCTA, 32, 64, 128,
+                          LBMGPU_TILE_STAGED3, LBMGPU_TILE_STAGED4, LBMGPU_TILE_RUNS};
     const int bpss[8] = {1, 2, 3, 4, 5, 6, 7, 8};
     double best = 1e30;
     int btx = b->tile, bbps = b->bps;
@@ -1992,6 +2053,7 @@ int lbmgpu_batch_autotune(lbmgpu_batch* b, int reps, int* threads_per_row, int* 
     for (int tx : tiles)
         for (int bps : bpss) {
             if ((tx == LBMGPU_TILE_ROWCTA || tx == LBMGPU_TILE_CHUNK) && bps != 1) continue;   // grid = rows / chunks
+            if (tx == LBMGPU_TILE_RUNS && bps > 3) continue;   // shared memory holds at most 2 resident
             const int grid = b->sms * bps;
             if (tx < 0) {
                 const int rc = set_bounds(b, grid);

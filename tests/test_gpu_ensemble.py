@@ -83,7 +83,8 @@ def test_ensemble_equals_members_alone(api, precision):
             assert_member_equals_alone(ens, i, p, Solver, [101, 129])
 
 
-@pytest.mark.parametrize("tiling", [(32, 1), (64, 3), (128, 8), (1, 1), (2, 1), (3, 4), (3, 7), (-3, 4), (-4, 2), (-3, 16)])
+@pytest.mark.parametrize("tiling", [(32, 1), (64, 3), (128, 8), (1, 1), (2, 1), (3, 4), (3, 7), (-3, 4), (-4, 2), (-3, 16),
+                                    (4, 1), (4, 2)])
 def test_ensemble_tiling_does_not_change_results(api, tiling):
     """Row kernel (tile > 0 threads per row) and staged kernel (tile = -2, -3
     stages), with few or many CTAs per SM: bit-identical to the lattices run
