@@ -290,7 +290,8 @@ def measure_lattice(p, prec, args, stream, dev, pg=None):
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(f"k_bulk:{args.workload}:{prec}")
+            tr = json.loads(tf.read_text())
+            traffic = tr.get(f"k_bulk_rows:{args.workload}:{prec}", tr.get(f"k_bulk:{args.workload}:{prec}"))
         except Exception:
             traffic = None
     return {
@@ -298,7 +299,8 @@ def measure_lattice(p, prec, args, stream, dev, pg=None):
         # kernels of the K-step window alone (the span's extra steps excluded)
         "launches": int(round(launches * args.steps / (args.steps + 2 * pre))),
         "clocks": clocks,
-        "roofline": {"bound": "hbm", "kernel": "k_bulk (collide-stream, AA, bulk nodes)",
+        "roofline": {"bound": "hbm", "kernel": "bulk collide-stream (k_bulk_rows on steps without sums, k_bulk "
+                                               "on the one in ten with sums; averaged)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "bytes_per_launch": bytes_per_launch, "launch_ms": kt["bulk"],

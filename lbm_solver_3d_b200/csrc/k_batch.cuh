@@ -400,6 +400,12 @@ __device__ __forceinline__ void span16(const void* p, size_t bytes, uintptr_t& s
 
 // velocity set by a runtime index (lanes of the producer take one direction each)
 __device__ __forceinline__ int c_opp_rt(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+__device__ __forceinline__ int c_cx_rt(int i) {
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) if (k == i) v = CX(k);
+    return v;
+}
 __device__ __forceinline__ int c_cy_rt(int i) {
     int v = 0;
 #pragma unroll
@@ -834,13 +840,14 @@ __host__ __device__ constexpr size_t rows_stage_bytes(int nx) {
     return (size_t)Q * nx * sizeof(typename S::T) + (size_t)nx;   // nx % 32 == 0: every part 16-byte aligned
 }
 
-// Populations of node x from a staged row (whole direction-rows of nx elements).
-template <class T>
+// Populations of node x from a staged row (whole direction-rows of nx elements;
+// odd steps read x - c_x, wrapped inside the row).
+template <class S>
 struct RowSrc {
-    const T* sb;
+    const typename S::T* sb;
     int nx, x;
-    template <class S, int PAR, class V>
-    __device__ __forceinline__ void load(const T*, unsigned, unsigned, const Nbr&, V* v) const {
+    template <class S_, int PAR, class V>
+    __device__ __forceinline__ void load(const typename S::T*, unsigned, unsigned, const Nbr&, V* v) const {
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             int xs = x;
@@ -853,7 +860,32 @@ struct RowSrc {
     }
 };
 
-template <class S, int PAR, bool SQ>
+// The producer warp's copies of one row into a stage (k_bulk_rows, _rows2):
+// lane i < 19 the direction-row of the state that the row's nodes read as
+// logical f_i (even step: A[i] of row (y, z); odd step: A[opp(i)] of row
+// (y - c_iy, z - c_iz), wrapped), lane 19 the row's flags; all whole rows.
+template <class S, int PAR>
+__device__ __forceinline__ void stage_row(const Lattice& L, const StreamArgs& a, int y, int z, unsigned char* sb,
+                                          uint64_t* full, int lane) {
+    using T = typename S::T;
+    const int nx = L.nx;
+    if (lane < Q) {
+        const int i = lane;
+        int ys = y, zs = z, arr = i;
+        if (PAR == 1) {
+            arr = c_opp_rt(i);
+            ys = y - c_cy_rt(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
+            zs = z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
+        }
+        const T* f = static_cast<const T*>(a.f);
+        bulk_g2s(sb + (size_t)i * nx * sizeof(T), f + (size_t)arr * L.N + (size_t)nx * (ys + (size_t)L.ny * zs),
+                 (unsigned)(nx * sizeof(T)), full);
+    } else if (lane == Q) {
+        bulk_g2s(sb + (size_t)Q * nx * sizeof(T), a.flag + (size_t)nx * (y + (size_t)L.ny * z), (unsigned)nx, full);
+    }
+}
+
+template <class S, int PAR, bool SQ, bool MACRO>
 __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_rows(const Lattice L, const StreamArgs a,
                                                                                  int nry, int nrows, int ylo, int zlo) {
     using T = typename S::T;
@@ -861,10 +893,136 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
     extern __shared__ __align__(128) unsigned char rows_raw[];
     __shared__ __align__(8) uint64_t full[NST], empty[NST];
     __shared__ ZoneBox zb;
+    __shared__ double red[NST][ROWS_MAX_NX / 32][4];   // the row's warp sums (summing steps)
+    __shared__ int cnt[NST];                            // update warps done with the row in stage q
     __shared__ volatile int s_abort;
     __shared__ int s_issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = L.nx, nupd = nx >> 5;
+    const size_t stage = rows_stage_bytes<S>(nx);
+    const bool sums_on = MACRO || a.do_mass;
+    if (tid == 0) {
+        for (int q = 0; q < NST; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], nupd);
+            cnt[q] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+        s_issued = 0;
+        if (SQ) zb = a.sq->zone[a.zslot];
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
+            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
+            if (k >= NST) {
+                int go = 1;
+                if (lane == 0) {
+                    const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
+                    if (!ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                    go = ok && !s_abort;
+                }
+                if (!__shfl_sync(0xffffffffu, go, 0)) break;
+            }
+            unsigned char* sb = rows_raw + (size_t)q * stage;
+            if (lane == 0) mbar_expect_tx(&full[q], (unsigned)stage);
+            __syncwarp();
+            stage_row<S, PAR>(L, a, ylo + r % nry, zlo + r / nry, sb, &full[q], lane);
+            if (lane == 0) s_issued = k + 1;
+            __syncwarp();
+        }
+    } else {
+        // ---------------- update threads ----------------
+        const int x = tid - 32, uw = warp - 1;
+        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
+            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
+            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                break;
+            }
+            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;   // lane 0's view, so the warp leaves together
+            const int y = ylo + r % nry, z = zlo + r / nry;
+            const unsigned char* sb = rows_raw + (size_t)q * stage;
+            const uint8_t fl = sb[(size_t)Q * nx * sizeof(T) + x];
+            bool active = (fl & (uint8_t)~NEAR_WALL) == 0;
+            // the zone test: y and z are the row's (uniform), x the node's
+            if (SQ && active && in_zone_axis(y, zb.lo[1], zb.w[1], L.ny, L.walls_y) &&
+                in_zone_axis(z, zb.lo[2], zb.w[2], L.nz, L.walls_z))
+                active = !in_zone_axis(x, zb.lo[0], zb.w[0], L.nx, false);
+            NodeSums sums;
+            if (active) {
+                const unsigned n = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+                update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, 0, MACRO, sums,
+                                                  RowSrc<S>{reinterpret_cast<const T*>(sb), nx, x});
+            }
+            if (sums_on) {
+                // the row's partial sums in k_bulk's order (a block of nx threads
+                // per row: each warp's shuffle tree, then the warps in order)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sums.fw[0] += __shfl_down_sync(0xffffffffu, sums.fw[0], o);
+                    sums.fw[1] += __shfl_down_sync(0xffffffffu, sums.fw[1], o);
+                    sums.fw[2] += __shfl_down_sync(0xffffffffu, sums.fw[2], o);
+                    sums.mass += __shfl_down_sync(0xffffffffu, sums.mass, o);
+                }
+                if (lane == 0) {
+                    double* c = red[q][uw];
+                    c[0] = sums.fw[0]; c[1] = sums.fw[1]; c[2] = sums.fw[2]; c[3] = sums.mass;
+                    __threadfence_block();
+                    if (atomicAdd(&cnt[q], 1) == nupd - 1) {   // the last warp done adds them up in order
+                        __threadfence_block();
+                        double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+                        for (int w = 0; w < nupd; ++w) {
+                            t0 += red[q][w][0]; t1 += red[q][w][1]; t2 += red[q][w][2]; t3 += red[q][w][3];
+                        }
+                        double* out = a.block_part + ((size_t)y + (size_t)L.ny * z) * BLOCK_PART;
+                        out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3;
+                        cnt[q] = 0;
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[q]);   // this warp is done with the stage (and red[q])
+        }
+    }
+    // after an abort, wait for the last copy armed into each stage (see k_bulk_staged)
+    __syncthreads();
+    if (tid == 0 && s_abort) {
+        const int issued = s_issued;
+        for (int q = 0; q < NST && q < issued; ++q) mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+//  k_bulk_rows2<S, PAR, SQ>: k_bulk_rows with two x-adjacent nodes per update
+//  thread (nx a multiple of 64), for the FP16 form, whose one-node kernel is
+//  bound by instruction issue rather than memory: the directions without an x
+//  shift are read from the stage as one 4-byte pair, and the results leave
+//  through pair_collide_store (paired conversions and 4-byte stores, the
+//  x-shifted directions exchanged between lanes), the second half of
+//  k_bulk_pair. Same staging, barriers, bounded waits and drain as k_bulk_rows.
+// ---------------------------------------------------------------------------
+template <class S> struct Rows2Cfg;
+template <> struct Rows2Cfg<StoreF16> { static constexpr int NST = 5, MINB = 4; };
+template <> struct Rows2Cfg<StoreF32> { static constexpr int NST = 3, MINB = 2; };
+
+template <class S, int PAR, bool SQ>
+__global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bulk_rows2(const Lattice L,
+                                                                                       const StreamArgs a, int nry,
+                                                                                       int nrows, int ylo, int zlo) {
+    using T = typename S::T;
+    constexpr int NST = Rows2Cfg<S>::NST;
+    extern __shared__ __align__(128) unsigned char rows_raw[];
+    __shared__ __align__(8) uint64_t full[NST], empty[NST];
+    __shared__ ZoneBox zb;
+    __shared__ volatile int s_abort;
+    __shared__ int s_issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nx = L.nx, nupd = nx >> 6;
     const size_t stage = rows_stage_bytes<S>(nx);
     if (tid == 0) {
         for (int q = 0; q < NST; ++q) {
@@ -879,8 +1037,7 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
     __syncthreads();
 
     if (warp == 0) {
-        // ---------------- producer ----------------
-        const T* f = static_cast<const T*>(a.f);
+        // ---------------- producer (as in k_bulk_rows) ----------------
         for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
             const int r = blockIdx.x + k * gridDim.x, q = k % NST;
             if (k >= NST) {
@@ -892,30 +1049,17 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
                 }
                 if (!__shfl_sync(0xffffffffu, go, 0)) break;
             }
-            const int y = ylo + r % nry, z = zlo + r / nry;
             unsigned char* sb = rows_raw + (size_t)q * stage;
             if (lane == 0) mbar_expect_tx(&full[q], (unsigned)stage);
             __syncwarp();
-            if (lane < Q) {
-                const int i = lane;
-                int ys = y, zs = z, arr = i;
-                if (PAR == 1) {
-                    arr = c_opp_rt(i);
-                    ys = y - c_cy_rt(i); if (ys < 0) ys += L.ny; else if (ys >= L.ny) ys -= L.ny;
-                    zs = z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
-                }
-                bulk_g2s(sb + (size_t)i * nx * sizeof(T), f + (size_t)arr * L.N + (size_t)nx * (ys + (size_t)L.ny * zs),
-                         (unsigned)(nx * sizeof(T)), &full[q]);
-            } else if (lane == Q) {
-                bulk_g2s(sb + (size_t)Q * nx * sizeof(T), a.flag + (size_t)nx * (y + (size_t)L.ny * z), (unsigned)nx,
-                         &full[q]);
-            }
+            stage_row<S, PAR>(L, a, ylo + r % nry, zlo + r / nry, sb, &full[q], lane);
             if (lane == 0) s_issued = k + 1;
             __syncwarp();
         }
     } else {
-        // ---------------- update threads ----------------
-        const int x = tid - 32;
+        // ---------------- update threads: nodes x0 = 2 t, x0 + 1 ----------------
+        T* __restrict__ fw = static_cast<T*>(a.f);
+        const int x0 = 2 * (tid - 32);
         for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
             const int r = blockIdx.x + k * gridDim.x, q = k % NST;
             const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
@@ -923,23 +1067,38 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
                 if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
                 break;
             }
-            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;   // lane 0's view, so the warp leaves together
+            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;
             const int y = ylo + r % nry, z = zlo + r / nry;
-            const unsigned char* sb = rows_raw + (size_t)q * stage;
-            const uint8_t fl = sb[(size_t)Q * nx * sizeof(T) + x];
-            bool active = (fl & (uint8_t)~NEAR_WALL) == 0;
-            if (SQ && active) active = !in_zone(L, zb, x, y, z);
-            if (active) {
-                const unsigned n = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
-                NodeSums sums;
-                update_node<S, PAR, false, false>(L, a, n, x, y, z, 0, 0, false, sums,
-                                                  RowSrc<T>{reinterpret_cast<const T*>(sb), nx, x});
+            const T* sb = reinterpret_cast<const T*>(rows_raw + (size_t)q * stage);
+            const uint8_t* sf = rows_raw + (size_t)q * stage + (size_t)Q * nx * sizeof(T);
+            bool act0 = (sf[x0] & (uint8_t)~NEAR_WALL) == 0, act1 = (sf[x0 + 1] & (uint8_t)~NEAR_WALL) == 0;
+            if (SQ && in_zone_axis(y, zb.lo[1], zb.w[1], L.ny, L.walls_y) &&
+                in_zone_axis(z, zb.lo[2], zb.w[2], L.nz, L.walls_z)) {
+                act0 = act0 && !in_zone_axis(x0, zb.lo[0], zb.w[0], nx, false);
+                act1 = act1 && !in_zone_axis(x0 + 1, zb.lo[0], zb.w[0], nx, false);
             }
+            const PairRow pr(L, x0, y, z, lane, act0, act1);
+            float d0[Q], d1[Q];
+#pragma unroll
+            for (int i = 0; i < Q; ++i) {
+                const T* rowi = sb + i * nx;
+                if (PAR == 0 || CX(i) == 0) {           // x0, x0 + 1: one aligned pair
+                    const float2 v = S::ld2(rowi + x0);
+                    d0[i] = v.x; d1[i] = v.y;
+                } else if (CX(i) > 0) {                 // x0 - 1 (wrapped), x0
+                    d0[i] = S::ld(rowi + (x0 == 0 ? nx - 1 : x0 - 1));
+                    d1[i] = S::ld(rowi + x0);
+                } else {                                // x0 + 1, x0 + 2 (wrapped)
+                    d0[i] = S::ld(rowi + x0 + 1);
+                    d1[i] = S::ld(rowi + (x0 + 2 == nx ? 0 : x0 + 2));
+                }
+            }
+            if (L.force_free) pair_collide_store<S, PAR, false>(L, a, fw, pr, d0, d1);
+            else pair_collide_store<S, PAR, true>(L, a, fw, pr, d0, d1);
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[q]);   // this warp is done with the stage
+            if (lane == 0) mbar_arrive(&empty[q]);
         }
     }
-    // after an abort, wait for the last copy armed into each stage (see k_bulk_staged)
     __syncthreads();
     if (tid == 0 && s_abort) {
         const int issued = s_issued;

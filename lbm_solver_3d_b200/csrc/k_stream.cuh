@@ -655,66 +655,45 @@ __global__ void __launch_bounds__(256, bulk_min_blocks<S>(DENSE)) k_bulk_flat(co
 // ---------------------------------------------------------------------------
 constexpr int PAIR_BLOCK = 128;
 
-template <class S, int PAR, bool SQ, bool FORCE>
-__global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, const StreamArgs a) {
-    using T = typename S::T;
-    pdl_wait();
-    pdl_launch_dependents();
-    const int y = blockIdx.y, z = blockIdx.z;
-    if (wall_row(L, y, z)) return;   // block-uniform: the wall-row launch owns this row
-    T* __restrict__ f = static_cast<T*>(a.f);
-    const unsigned N = L.N;
-    const int lane = threadIdx.x & 31;
-    const int x0 = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const unsigned row = (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
-    const unsigned n0 = row + (unsigned)x0;
-    bool act0 = (a.flag[n0] & (uint8_t)~NEAR_WALL) == 0;
-    bool act1 = (a.flag[n0 + 1] & (uint8_t)~NEAR_WALL) == 0;
-    if (SQ) {
-        const ZoneBox zb = a.sq->zone[a.zslot];
-        act0 = act0 && !in_zone(L, zb, x0, y, z);
-        act1 = act1 && !in_zone(L, zb, x0 + 1, y, z);
+// A thread's pair of nodes (x0, x0 + 1) in row (y, z), with its neighbours in
+// the warp along x: has_prev / has_next = the lane before / after holds the
+// pair before / after in the same row (not across a warp or the periodic
+// boundary), prev_act1 / next_act0 = that lane's adjacent node is updated by
+// the bulk; xm / xp = x0 - 1 and x0 + 2 wrapped.
+struct PairRow {
+    unsigned row, n0;
+    int x0, xm, xp, y, z;
+    int yp, ym, zp, zm;   // row offsets of the y/z neighbours (periodic wrap as in Nbr)
+    bool act0, act1, prev_act1, next_act0, has_prev, has_next;
+    __device__ __forceinline__ PairRow(const Lattice& L, int x0_, int y_, int z_, int lane, bool a0, bool a1)
+        : x0(x0_), y(y_), z(z_), act0(a0), act1(a1) {
+        row = (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
+        n0 = row + (unsigned)x0;
+        has_prev = lane > 0 && x0 > 0;
+        has_next = lane < 31 && x0 + 2 < L.nx;
+        prev_act1 = __shfl_up_sync(0xffffffffu, act1, 1) && has_prev;
+        next_act0 = __shfl_down_sync(0xffffffffu, act0, 1) && has_next;
+        xm = x0 == 0 ? L.nx - 1 : x0 - 1;
+        xp = x0 + 2 == L.nx ? 0 : x0 + 2;
+        yp = (y == L.ny - 1) ? (1 - L.ny) * L.nx : L.nx;
+        ym = (y == 0) ? (L.ny - 1) * L.nx : -L.nx;
+        zp = (z == L.nz - 1) ? (1 - L.nz) * (int)L.nxy : (int)L.nxy;
+        zm = (z == 0) ? (L.nz - 1) * (int)L.nxy : -(int)L.nxy;
     }
-    // lanes whose pair neighbour in x sits in the same warp (no periodic wrap)
-    const bool has_prev = lane > 0 && x0 > 0;
-    const bool has_next = lane < 31 && x0 + 2 < L.nx;
-    const bool prev_act1 = __shfl_up_sync(0xffffffffu, act1, 1) && has_prev;
-    const bool next_act0 = __shfl_down_sync(0xffffffffu, act0, 1) && has_next;
-    const int xm = x0 == 0 ? L.nx - 1 : x0 - 1;        // x0 - 1, wrapped
-    const int xp = x0 + 2 == L.nx ? 0 : x0 + 2;        // x0 + 2, wrapped
-    // row offsets of the y/z neighbours (periodic wrap as in Nbr)
-    const int yp = (y == L.ny - 1) ? (1 - L.ny) * L.nx : L.nx;
-    const int ym = (y == 0) ? (L.ny - 1) * L.nx : -L.nx;
-    const int zp = (z == L.nz - 1) ? (1 - L.nz) * (int)L.nxy : (int)L.nxy;
-    const int zm = (z == 0) ? (L.nz - 1) * (int)L.nxy : -(int)L.nxy;
-    auto ryz = [&](int i) {   // row offset of n + c_i in y and z
+    __device__ __forceinline__ int ryz(int i) const {   // row offset of n + c_i in y and z
         return (CY(i) > 0 ? yp : (CY(i) < 0 ? ym : 0)) + (CZ(i) > 0 ? zp : (CZ(i) < 0 ? zm : 0));
-    };
-
-    // ---- loads: logical f_i of both nodes ----
-    float d0[Q], d1[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        if (PAR == 0) {
-            const float2 q = S::ld2(f + (size_t)i * N + n0);
-            d0[i] = q.x; d1[i] = q.y;
-        } else {
-            const int o = OPP(i);                              // read A[o][n + c_o]
-            const T* rowp = f + (size_t)o * N + (size_t)((int)row + ryz(o));
-            const float2 q = S::ld2(rowp + x0);
-            if (CX(o) == 0) {
-                d0[i] = q.x; d1[i] = q.y;
-            } else if (CX(o) < 0) {                            // source x - 1
-                const float up = __shfl_up_sync(0xffffffffu, q.y, 1);
-                d0[i] = has_prev ? up : S::ld(rowp + xm);
-                d1[i] = q.x;
-            } else {                                           // source x + 1
-                const float dn = __shfl_down_sync(0xffffffffu, q.x, 1);
-                d0[i] = q.y;
-                d1[i] = has_next ? dn : S::ld(rowp + xp);
-            }
-        }
     }
+};
+
+// Collide and store of a thread's two nodes (the second half of k_bulk_pair,
+// shared with the staged two-node kernel): d0, d1 are the 19 logical stored
+// numbers of x0 and x0 + 1. Every lane of the warp calls it (the stores
+// shuffle the x-shifted values between lanes).
+template <class S, int PAR, bool FORCE>
+__device__ __forceinline__ void pair_collide_store(const Lattice& L, const StreamArgs& a, typename S::T* __restrict__ f,
+                                                   const PairRow& pr, float* d0, float* d1) {
+    using T = typename S::T;
+    const unsigned N = L.N;
     if (a.apply_corr) {
         const double corr = a.sq->corr_d;
 #pragma unroll
@@ -733,31 +712,32 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, co
     const AR uF0 = u0 * C::F(L, 0) + v0 * C::F(L, 1) + w0 * C::F(L, 2);
     const AR uF1 = u1 * C::F(L, 0) + v1 * C::F(L, 1) + w1 * C::F(L, 2);
     const AR sr0 = (AR)S::SC * rho0, sr1 = (AR)S::SC * rho1;
+    const int x0 = pr.x0;
+    const bool act0 = pr.act0, act1 = pr.act1;
 
-    // ---- stores: post-collision value of direction i to its slot ----
-    // (a0, a1) = the values of nodes x0, x0 + 1 for direction i, already
-    // rounded to the FP32 they are stored through
+    // post-collision value of direction i to its slot; (a0, a1) = the values
+    // of nodes x0, x0 + 1, already rounded to the FP32 they are stored through
     auto put = [&](int i, float a0, float a1) {
         if (PAR == 0) {                                        // A[opp(i)][n]
-            T* p = f + (size_t)OPP(i) * N + n0;
+            T* p = f + (size_t)OPP(i) * N + pr.n0;
             if (act0 && act1) S::st2(p, a0, a1);
             else { if (act0) S::st(p, a0); if (act1) S::st(p + 1, a1); }
             return;
         }
-        T* rowp = f + (size_t)i * N + (size_t)((int)row + ryz(i));   // A[i][n + c_i]
+        T* rowp = f + (size_t)i * N + (size_t)((int)pr.row + pr.ryz(i));   // A[i][n + c_i]
         if (CX(i) == 0) {
             if (act0 && act1) S::st2(rowp + x0, a0, a1);
             else { if (act0) S::st(rowp + x0, a0); if (act1) S::st(rowp + x0 + 1, a1); }
         } else if (CX(i) > 0) {                                // targets x0 + 1, x0 + 2
             const float pv = __shfl_up_sync(0xffffffffu, a1, 1);
-            if (prev_act1 && act0) S::st2(rowp + x0, pv, a0);
-            else { if (prev_act1) S::st(rowp + x0, pv); if (act0) S::st(rowp + x0 + 1, a0); }
-            if (!has_next && act1) S::st(rowp + xp, a1);
+            if (pr.prev_act1 && act0) S::st2(rowp + x0, pv, a0);
+            else { if (pr.prev_act1) S::st(rowp + x0, pv); if (act0) S::st(rowp + x0 + 1, a0); }
+            if (!pr.has_next && act1) S::st(rowp + pr.xp, a1);
         } else {                                               // targets x0 - 1, x0
             const float nv = __shfl_down_sync(0xffffffffu, a0, 1);
-            if (act1 && next_act0) S::st2(rowp + x0, a1, nv);
-            else { if (act1) S::st(rowp + x0, a1); if (next_act0) S::st(rowp + x0 + 1, nv); }
-            if (!has_prev && act0) S::st(rowp + xm, a0);
+            if (act1 && pr.next_act0) S::st2(rowp + x0, a1, nv);
+            else { if (act1) S::st(rowp + x0, a1); if (pr.next_act0) S::st(rowp + x0 + 1, nv); }
+            if (!pr.has_prev && act0) S::st(rowp + pr.xm, a0);
         }
     };
     put(0, (float)rest_post<S, FORCE>(L, (AR)d0[0], dr0, sr0, k0, uF0),
@@ -772,6 +752,54 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, co
         put(i, (float)a0i, (float)a1i);
         put(i + 1, (float)a0o, (float)a1o);
     }
+}
+
+template <class S, int PAR, bool SQ, bool FORCE>
+__global__ void __launch_bounds__(PAIR_BLOCK, 4) k_bulk_pair(const Lattice L, const StreamArgs a) {
+    using T = typename S::T;
+    pdl_wait();
+    pdl_launch_dependents();
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (wall_row(L, y, z)) return;   // block-uniform: the wall-row launch owns this row
+    T* __restrict__ f = static_cast<T*>(a.f);
+    const unsigned N = L.N;
+    const int lane = threadIdx.x & 31;
+    const int x0 = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const unsigned n0 = (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z) + (unsigned)x0;
+    bool act0 = (a.flag[n0] & (uint8_t)~NEAR_WALL) == 0;
+    bool act1 = (a.flag[n0 + 1] & (uint8_t)~NEAR_WALL) == 0;
+    if (SQ) {
+        const ZoneBox zb = a.sq->zone[a.zslot];
+        act0 = act0 && !in_zone(L, zb, x0, y, z);
+        act1 = act1 && !in_zone(L, zb, x0 + 1, y, z);
+    }
+    const PairRow pr(L, x0, y, z, lane, act0, act1);
+
+    // ---- loads: logical f_i of both nodes ----
+    float d0[Q], d1[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (PAR == 0) {
+            const float2 q = S::ld2(f + (size_t)i * N + n0);
+            d0[i] = q.x; d1[i] = q.y;
+        } else {
+            const int o = OPP(i);                              // read A[o][n + c_o]
+            const T* rowp = f + (size_t)o * N + (size_t)((int)pr.row + pr.ryz(o));
+            const float2 q = S::ld2(rowp + x0);
+            if (CX(o) == 0) {
+                d0[i] = q.x; d1[i] = q.y;
+            } else if (CX(o) < 0) {                            // source x - 1
+                const float up = __shfl_up_sync(0xffffffffu, q.y, 1);
+                d0[i] = pr.has_prev ? up : S::ld(rowp + pr.xm);
+                d1[i] = q.x;
+            } else {                                           // source x + 1
+                const float dn = __shfl_down_sync(0xffffffffu, q.x, 1);
+                d0[i] = q.y;
+                d1[i] = pr.has_next ? dn : S::ld(rowp + pr.xp);
+            }
+        }
+    }
+    pair_collide_store<S, PAR, FORCE>(L, a, f, pr, d0, d1);
 }
 
 // ---------------------------------------------------------------------------

@@ -25,6 +25,7 @@ struct StreamGeom {
     // (rows_grid = 0: not used), interior rows nry x (rows_n / nry) from (ylo, zlo)
     unsigned rows_grid = 0;
     int rows_nry = 0, rows_n = 0, rows_ylo = 0, rows_zlo = 0;
+    bool rows_pairs = false;   // two nodes per update thread (k_bulk_rows2)
 };
 
 struct SqArgs;
@@ -80,7 +81,7 @@ struct Launchers {
     // one warp per 32-node chunk (k_bulk_chunk, then k_fold_chunks when summing)
     void (*batch_chunk)(int par, bool macro, bool sums, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
     int (*chunkp_ctas_per_sm)();   // resident CTAs per SM of the persistent chunk kernel
-    int (*rows_ctas_per_sm)(int nx);   // resident CTAs per SM of k_bulk_rows for rows of nx nodes
+    int (*rows_ctas_per_sm)(int nx, bool pairs);   // resident CTAs per SM of k_bulk_rows(2) for rows of nx nodes
     // rows away from walls in runs staged through shared memory (k_bulk_runs, steps without sums)
     void (*batch_runs)(int par, int grid, const BatchArgs& b, BatchStep st, cudaStream_t s);
     int runs_max_nodes;                // nodes per run

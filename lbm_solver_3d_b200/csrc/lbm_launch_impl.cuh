@@ -13,12 +13,24 @@ namespace lbmgpu {
 
 template <class S>
 static size_t rows_smem(int nx) { return (size_t)RowsCfg<S>::NST * rows_stage_bytes<S>(nx); }
+template <class S>
+static size_t rows2_smem(int nx) {
+    if constexpr (S::shifted) return (size_t)Rows2Cfg<S>::NST * rows_stage_bytes<S>(nx);
+    else return 0;
+}
 
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
-    if (!MACRO && !a.do_mass && g.rows_grid) {   // no sums this step: rows staged in shared memory
-        k_bulk_rows<S, PAR, SQ><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(L, a, g.rows_nry, g.rows_n,
-                                                                                  g.rows_ylo, g.rows_zlo);
+    if (g.rows_grid) {   // rows staged in shared memory (every step; sums in k_bulk's order)
+        if constexpr (S::shifted && !MACRO) {
+            if (g.rows_pairs && !a.do_mass) {   // no sums this step: two nodes per update thread
+                k_bulk_rows2<S, PAR, SQ><<<g.rows_grid, 32 + L.nx / 2, rows2_smem<S>(L.nx), st>>>(
+                    L, a, g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo);
+                return;
+            }
+        }
+        k_bulk_rows<S, PAR, SQ, MACRO><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(
+            L, a, g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo);
         return;
     }
     if constexpr (S::shifted && !MACRO) {
@@ -268,12 +280,17 @@ static void batch_runs_launch(int par, int grid, const BatchArgs& b, BatchStep s
 }
 
 template <class S>
-static int rows_occupancy(int nx) {
+static int rows_occupancy(int nx, bool pairs) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows<S, 0, true>, 32 + nx, rows_smem<S>(nx)) !=
-        cudaSuccess)
-        return 0;
-    return n;
+    cudaError_t e;
+    if constexpr (S::shifted) {
+        if (pairs) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows2<S, 0, true>, 32 + nx / 2, rows2_smem<S>(nx));
+            return e == cudaSuccess ? n : 0;
+        }
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows<S, 0, true, false>, 32 + nx, rows_smem<S>(nx));
+    return e == cudaSuccess ? n : 0;
 }
 
 template <class S>
@@ -285,8 +302,18 @@ static cudaError_t prepare_launch() {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, runs_smem);
         if (e != cudaSuccess) return e;
     }
+    if constexpr (S::shifted) {
+        const int r2 = (int)rows2_smem<S>(ROWS_MAX_NX);
+        for (auto fn : {k_bulk_rows2<S, 0, false>, k_bulk_rows2<S, 0, true>, k_bulk_rows2<S, 1, false>,
+                        k_bulk_rows2<S, 1, true>}) {
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, r2);
+            if (e != cudaSuccess) return e;
+        }
+    }
     const int rs = (int)rows_smem<S>(ROWS_MAX_NX);
-    for (auto fn : {k_bulk_rows<S, 0, false>, k_bulk_rows<S, 0, true>, k_bulk_rows<S, 1, false>, k_bulk_rows<S, 1, true>}) {
+    for (auto fn : {k_bulk_rows<S, 0, false, false>, k_bulk_rows<S, 0, true, false>, k_bulk_rows<S, 1, false, false>,
+                    k_bulk_rows<S, 1, true, false>, k_bulk_rows<S, 0, false, true>, k_bulk_rows<S, 0, true, true>,
+                    k_bulk_rows<S, 1, false, true>, k_bulk_rows<S, 1, true, true>}) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, rs);
         if (e != cudaSuccess) return e;
     }

@@ -154,12 +154,15 @@ const Launchers* launchers_for(int prec) {
 size_t esize_for(int prec) { return prec == LBMGPU_FP64 ? 8 : (prec == LBMGPU_FP32 ? 4 : 2); }
 
 // The bulk kernel of steps without sums, where the lattice allows a choice:
-// LBMGPU_BULK=rows (rows staged in shared memory, the default), pair (two
-// nodes per thread, shifted forms) or node (one node per thread). The results
-// are the same bit for bit; the variable exists to compare their speed.
+// LBMGPU_BULK=rows (rows staged in shared memory, the default: two nodes per
+// update thread in FP16 storage, one otherwise), rows1 (staged, one node per
+// thread in every form), pair (two nodes per thread loaded from global memory,
+// shifted forms) or node (one node per thread). The results are the same bit
+// for bit; the variable exists to compare their speed.
 int bulk_kind() {
     const char* e = std::getenv("LBMGPU_BULK");
     if (!e || !*e || !std::strcmp(e, "rows")) return 2;
+    if (!std::strcmp(e, "rows1")) return 3;
     if (!std::strcmp(e, "pair")) return 1;
     return 0;
 }
@@ -735,9 +738,10 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
         // nx a multiple of 32 up to 256: rows staged in shared memory
         // (k_bulk_rows), a persistent grid of the CTAs that fit on the SMs
         h->geom.rows_grid = 0;
-        if (p->nx % 32 == 0 && p->nx <= ROWS_MAX_NX && rows > 0 && planes > 0 && bulk_kind() == 2) {
+        if (p->nx % 32 == 0 && p->nx <= ROWS_MAX_NX && rows > 0 && planes > 0 && bulk_kind() >= 2) {
             int sms = 0, dev = p->device;
-            const int per_sm = h->lz->rows_ctas_per_sm(p->nx);
+            h->geom.rows_pairs = p->precision == LBMGPU_FP16 && p->nx % 64 == 0 && bulk_kind() == 2;
+            const int per_sm = h->lz->rows_ctas_per_sm(p->nx, h->geom.rows_pairs);
             if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && per_sm > 0) {
                 h->geom.rows_nry = rows;
                 h->geom.rows_n = rows * planes;
