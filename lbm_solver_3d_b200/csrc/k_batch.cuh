@@ -813,13 +813,20 @@ __global__ void __launch_bounds__(RUNS_THREADS, 2) k_bulk_runs(const Lattice* __
 //  of all 19 directions (plus the row's flags) in flight in shared memory.
 //
 //  CTA = one producer warp + nx update threads (nx a multiple of 32, at most
-//  ROWS_MAX_NX), persistent over the interior rows r = blockIdx.x + k *
-//  gridDim.x (y = ylo + r % nry, z = zlo + r / nry).
-//    producer   per row: waits for the stage to be free (empty barrier), then
+//  ROWS_MAX_NX), persistent over the interior rows (y = ylo + r % nry,
+//  z = zlo + r / nry), which the producers claim one at a time from a counter
+//  (RowsWork): a CTA that starts late, or shares its SM with other kernels,
+//  takes fewer rows instead of ending late. CTAs that find themselves on one
+//  of the `reserve` SMs with the lowest %smid leave at once, so the zone and
+//  squirmer kernels of the second stream always find whole SMs free while
+//  this grid runs (a grid that held every SM would put them after it).
+//    producer   per row: claims the row, waits for the stage to be free
+//               (empty barrier), publishes the row number, then
 //               lane i < 19 copies direction-row i of the state -- A[i] of row
 //               (y, z) on an even step, A[opp(i)] of row (y - c_iy, z - c_iz)
 //               on an odd step, always a whole row, 16-byte aligned -- and
 //               lane 19 the row's flags, completing on the full barrier;
+//               when the rows are used up it publishes -1 (a plain arrive);
 //    update     thread x waits for the row (full barrier), reads its 19
 //               logical populations from the stage (odd step: x - c_ix,
 //               wrapped, inside the staged row), updates the node with the
@@ -838,6 +845,23 @@ template <> struct RowsCfg<StoreF16> { static constexpr int NST = 6, MINB = 3; }
 template <class S>
 __host__ __device__ constexpr size_t rows_stage_bytes(int nx) {
     return (size_t)Q * nx * sizeof(typename S::T) + (size_t)nx;   // nx % 32 == 0: every part 16-byte aligned
+}
+
+// The interior rows of one launch and how CTAs share them. claim[0] is the
+// next unclaimed row, claim[1] the CTAs that have finished; the last CTA to
+// finish sets both back to 0 for the next launch, which stream order keeps
+// after this one.
+struct RowsWork {
+    int nry, nrows, ylo, zlo;   // rows nry x (nrows / nry) from (ylo, zlo)
+    int reserve;                // CTAs on SMs with %smid < reserve take no rows
+    int cap;                    // rows one CTA takes at most (0: no limit)
+    int* claim;
+};
+
+__device__ __forceinline__ unsigned sm_id() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
 }
 
 // Populations of node x from a staged row (whole direction-rows of nx elements;
@@ -885,22 +909,106 @@ __device__ __forceinline__ void stage_row(const Lattice& L, const StreamArgs& a,
     }
 }
 
-template <class S, int PAR, bool SQ, bool MACRO>
+// A CTA on a reserved SM takes no rows, and any other takes at most w.cap --
+// except the grid's last CTA, which takes whatever is left, so that every row
+// is done whatever the grid's placement (the claim counter lets one CTA finish
+// them all). Uniform over the CTA.
+__device__ __forceinline__ bool rows_idle(const RowsWork& w) {
+    return (int)sm_id() < w.reserve && blockIdx.x + 1 < gridDim.x;
+}
+__device__ __forceinline__ int rows_cap(const RowsWork& w) { return blockIdx.x + 1 < gridDim.x ? w.cap : 0; }
+
+// The producer loop shared by k_bulk_rows and k_bulk_rows2 (warp 0): claim a
+// row, wait for its stage, publish it in rowid[q] and stage it; -1 ends the
+// consumers' loop. Returns with s_issued = stages armed with copies.
+template <class S, int PAR, int NST>
+__device__ __forceinline__ void rows_produce(const Lattice& L, const StreamArgs& a, const RowsWork& w,
+                                             unsigned char* raw, size_t stage, uint64_t* full, uint64_t* empty,
+                                             int* rowid, volatile int& s_abort, int& s_issued, int lane) {
+    const int cap = rows_cap(w);
+    for (int k = 0;; ++k) {
+        const int q = k % NST;
+        int r = w.nrows;
+        if (lane == 0 && (cap == 0 || k < cap)) r = atomicAdd(w.claim, 1);   // before the wait: its latency overlaps it
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (k >= NST) {
+            int go = 1;
+            if (lane == 0) {
+                const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
+                if (!ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                go = ok && !s_abort;
+            }
+            if (!__shfl_sync(0xffffffffu, go, 0)) return;
+        }
+        if (r >= w.nrows) {   // no rows left: the consumers stop at this stage
+            if (lane == 0) { rowid[q] = -1; mbar_arrive(&full[q]); }
+            return;
+        }
+        unsigned char* sb = raw + (size_t)q * stage;
+        if (lane == 0) { rowid[q] = r; mbar_expect_tx(&full[q], (unsigned)stage); }   // the arrive releases rowid[q]
+        __syncwarp();
+        stage_row<S, PAR>(L, a, w.ylo + r % w.nry, w.zlo + r / w.nry, sb, &full[q], lane);
+        if (lane == 0) s_issued = k + 1;
+        __syncwarp();
+    }
+}
+
+// The consumers' wait for stage k: the row staged there, or -1 to leave (no
+// rows left, or an abort, whose watchdog status this sets).
+template <int NST>
+__device__ __forceinline__ int rows_next(const StreamArgs& a, uint64_t* full, const int* rowid,
+                                         volatile int& s_abort, int k, int lane) {
+    const int q = k % NST;
+    const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+    if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+        return -1;
+    }
+    if (__shfl_sync(0xffffffffu, s_abort, 0)) return -1;   // lane 0's view, so the warp leaves together
+    return __shfl_sync(0xffffffffu, rowid[q], 0);
+}
+
+// The end of a rows kernel: after an abort one thread waits (bounded) for the
+// last copy armed into each stage, then the CTA counts itself done; the last
+// one resets the claim counter.
+template <int NST>
+__device__ __forceinline__ void rows_finish(const RowsWork& w, uint64_t* full, volatile int& s_abort, int s_issued,
+                                            int tid) {
+    __syncthreads();
+    if (tid == 0) {
+        if (s_abort) {
+            const int issued = s_issued;
+            for (int q = 0; q < NST && q < issued; ++q)
+                mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
+        }
+        __threadfence();
+        if (atomicAdd(w.claim + 1, 1) == (int)gridDim.x - 1) {
+            w.claim[0] = 0;
+            w.claim[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// SUMS: the step forms the rows' partial sums (a mass-correction step, or
+// MACRO); steps without sums run an instantiation without that code.
+template <class S, int PAR, bool SQ, bool MACRO, bool SUMS>
 __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_rows(const Lattice L, const StreamArgs a,
-                                                                                 int nry, int nrows, int ylo, int zlo) {
+                                                                                 const RowsWork w) {
     using T = typename S::T;
     constexpr int NST = RowsCfg<S>::NST;
     extern __shared__ __align__(128) unsigned char rows_raw[];
     __shared__ __align__(8) uint64_t full[NST], empty[NST];
     __shared__ ZoneBox zb;
-    __shared__ double red[NST][ROWS_MAX_NX / 32][4];   // the row's warp sums (summing steps)
-    __shared__ int cnt[NST];                            // update warps done with the row in stage q
+    __shared__ double red[SUMS ? NST : 1][ROWS_MAX_NX / 32][4];   // the row's warp sums (summing steps)
+    __shared__ int cnt[NST];                                       // update warps done with the row in stage q
+    __shared__ int rowid[NST];                                     // the row in stage q (-1: none left)
     __shared__ volatile int s_abort;
     __shared__ int s_issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = L.nx, nupd = nx >> 5;
     const size_t stage = rows_stage_bytes<S>(nx);
-    const bool sums_on = MACRO || a.do_mass;
+    const bool idle = rows_idle(w);
     if (tid == 0) {
         for (int q = 0; q < NST; ++q) {
             mbar_init(&full[q], 1);
@@ -914,38 +1022,17 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
     }
     __syncthreads();
 
-    if (warp == 0) {
-        // ---------------- producer ----------------
-        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
-            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
-            if (k >= NST) {
-                int go = 1;
-                if (lane == 0) {
-                    const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
-                    if (!ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
-                    go = ok && !s_abort;
-                }
-                if (!__shfl_sync(0xffffffffu, go, 0)) break;
-            }
-            unsigned char* sb = rows_raw + (size_t)q * stage;
-            if (lane == 0) mbar_expect_tx(&full[q], (unsigned)stage);
-            __syncwarp();
-            stage_row<S, PAR>(L, a, ylo + r % nry, zlo + r / nry, sb, &full[q], lane);
-            if (lane == 0) s_issued = k + 1;
-            __syncwarp();
-        }
+    if (idle) {
+    } else if (warp == 0) {
+        rows_produce<S, PAR, NST>(L, a, w, rows_raw, stage, full, empty, rowid, s_abort, s_issued, lane);
     } else {
         // ---------------- update threads ----------------
         const int x = tid - 32, uw = warp - 1;
-        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
-            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
-            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
-            if (!__all_sync(0xffffffffu, ok)) {
-                if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
-                break;
-            }
-            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;   // lane 0's view, so the warp leaves together
-            const int y = ylo + r % nry, z = zlo + r / nry;
+        for (int k = 0;; ++k) {
+            const int r = rows_next<NST>(a, full, rowid, s_abort, k, lane);
+            if (r < 0) break;
+            const int q = k % NST;
+            const int y = w.ylo + r % w.nry, z = w.zlo + r / w.nry;
             const unsigned char* sb = rows_raw + (size_t)q * stage;
             const uint8_t fl = sb[(size_t)Q * nx * sizeof(T) + x];
             bool active = (fl & (uint8_t)~NEAR_WALL) == 0;
@@ -959,7 +1046,7 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
                 update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, 0, MACRO, sums,
                                                   RowSrc<S>{reinterpret_cast<const T*>(sb), nx, x});
             }
-            if (sums_on) {
+            if constexpr (SUMS) {
                 // the row's partial sums in k_bulk's order (a block of nx threads
                 // per row: each warp's shuffle tree, then the warps in order)
 #pragma unroll
@@ -976,8 +1063,8 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
                     if (atomicAdd(&cnt[q], 1) == nupd - 1) {   // the last warp done adds them up in order
                         __threadfence_block();
                         double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-                        for (int w = 0; w < nupd; ++w) {
-                            t0 += red[q][w][0]; t1 += red[q][w][1]; t2 += red[q][w][2]; t3 += red[q][w][3];
+                        for (int v = 0; v < nupd; ++v) {
+                            t0 += red[q][v][0]; t1 += red[q][v][1]; t2 += red[q][v][2]; t3 += red[q][v][3];
                         }
                         double* out = a.block_part + ((size_t)y + (size_t)L.ny * z) * BLOCK_PART;
                         out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3;
@@ -989,12 +1076,7 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
             if (lane == 0) mbar_arrive(&empty[q]);   // this warp is done with the stage (and red[q])
         }
     }
-    // after an abort, wait for the last copy armed into each stage (see k_bulk_staged)
-    __syncthreads();
-    if (tid == 0 && s_abort) {
-        const int issued = s_issued;
-        for (int q = 0; q < NST && q < issued; ++q) mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
-    }
+    rows_finish<NST>(w, full, s_abort, s_issued, tid);
 }
 
 // ---------------------------------------------------------------------------
@@ -1012,18 +1094,20 @@ template <> struct Rows2Cfg<StoreF32> { static constexpr int NST = 3, MINB = 2; 
 
 template <class S, int PAR, bool SQ>
 __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bulk_rows2(const Lattice L,
-                                                                                       const StreamArgs a, int nry,
-                                                                                       int nrows, int ylo, int zlo) {
+                                                                                       const StreamArgs a,
+                                                                                       const RowsWork w) {
     using T = typename S::T;
     constexpr int NST = Rows2Cfg<S>::NST;
     extern __shared__ __align__(128) unsigned char rows_raw[];
     __shared__ __align__(8) uint64_t full[NST], empty[NST];
     __shared__ ZoneBox zb;
+    __shared__ int rowid[NST];
     __shared__ volatile int s_abort;
     __shared__ int s_issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = L.nx, nupd = nx >> 6;
     const size_t stage = rows_stage_bytes<S>(nx);
+    const bool idle = rows_idle(w);
     if (tid == 0) {
         for (int q = 0; q < NST; ++q) {
             mbar_init(&full[q], 1);
@@ -1036,39 +1120,18 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
     }
     __syncthreads();
 
-    if (warp == 0) {
-        // ---------------- producer (as in k_bulk_rows) ----------------
-        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
-            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
-            if (k >= NST) {
-                int go = 1;
-                if (lane == 0) {
-                    const bool ok = mbar_wait(&empty[q], (uint32_t)((k / NST - 1) & 1));
-                    if (!ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
-                    go = ok && !s_abort;
-                }
-                if (!__shfl_sync(0xffffffffu, go, 0)) break;
-            }
-            unsigned char* sb = rows_raw + (size_t)q * stage;
-            if (lane == 0) mbar_expect_tx(&full[q], (unsigned)stage);
-            __syncwarp();
-            stage_row<S, PAR>(L, a, ylo + r % nry, zlo + r / nry, sb, &full[q], lane);
-            if (lane == 0) s_issued = k + 1;
-            __syncwarp();
-        }
+    if (idle) {
+    } else if (warp == 0) {
+        rows_produce<S, PAR, NST>(L, a, w, rows_raw, stage, full, empty, rowid, s_abort, s_issued, lane);
     } else {
         // ---------------- update threads: nodes x0 = 2 t, x0 + 1 ----------------
         T* __restrict__ fw = static_cast<T*>(a.f);
         const int x0 = 2 * (tid - 32);
-        for (int k = 0; (int)blockIdx.x + k * (int)gridDim.x < nrows; ++k) {
-            const int r = blockIdx.x + k * gridDim.x, q = k % NST;
-            const bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
-            if (!__all_sync(0xffffffffu, ok)) {
-                if (lane == 0 && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
-                break;
-            }
-            if (__shfl_sync(0xffffffffu, s_abort, 0)) break;
-            const int y = ylo + r % nry, z = zlo + r / nry;
+        for (int k = 0;; ++k) {
+            const int r = rows_next<NST>(a, full, rowid, s_abort, k, lane);
+            if (r < 0) break;
+            const int q = k % NST;
+            const int y = w.ylo + r % w.nry, z = w.zlo + r / w.nry;
             const T* sb = reinterpret_cast<const T*>(rows_raw + (size_t)q * stage);
             const uint8_t* sf = rows_raw + (size_t)q * stage + (size_t)Q * nx * sizeof(T);
             bool act0 = (sf[x0] & (uint8_t)~NEAR_WALL) == 0, act1 = (sf[x0 + 1] & (uint8_t)~NEAR_WALL) == 0;
@@ -1099,11 +1162,7 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
             if (lane == 0) mbar_arrive(&empty[q]);
         }
     }
-    __syncthreads();
-    if (tid == 0 && s_abort) {
-        const int issued = s_issued;
-        for (int q = 0; q < NST && q < issued; ++q) mbar_wait(&full[q], (uint32_t)(((issued - q + NST - 1) / NST - 1) & 1));
-    }
+    rows_finish<NST>(w, full, s_abort, s_issued, tid);
 }
 
 // One CTA per zone block of every member: zblocks lists the (member, block)

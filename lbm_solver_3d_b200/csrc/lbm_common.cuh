@@ -222,6 +222,7 @@ struct StreamArgs {
     int zslot;                    // zone slot of this step
     int do_mass;                  // sum the stored populations (a correction step)
     int apply_corr;               // add the pending correction on load (after one)
+    int* row_claim;               // staged-row bulk: row counter and CTAs done (RowsWork)
 };
 
 // ---- ensembles (k_batch.cuh) -------------------------------------------------

@@ -22,15 +22,17 @@ static size_t rows2_smem(int nx) {
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
     if (g.rows_grid) {   // rows staged in shared memory (every step; sums in k_bulk's order)
+        const RowsWork w{g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo, g.rows_reserve, g.rows_cap, a.row_claim};
         if constexpr (S::shifted && !MACRO) {
             if (g.rows_pairs && !a.do_mass) {   // no sums this step: two nodes per update thread
-                k_bulk_rows2<S, PAR, SQ><<<g.rows_grid, 32 + L.nx / 2, rows2_smem<S>(L.nx), st>>>(
-                    L, a, g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo);
+                k_bulk_rows2<S, PAR, SQ><<<g.rows_grid, 32 + L.nx / 2, rows2_smem<S>(L.nx), st>>>(L, a, w);
                 return;
             }
         }
-        k_bulk_rows<S, PAR, SQ, MACRO><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(
-            L, a, g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo);
+        if (MACRO || a.do_mass)
+            k_bulk_rows<S, PAR, SQ, MACRO, true><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(L, a, w);
+        else
+            k_bulk_rows<S, PAR, SQ, false, false><<<g.rows_grid, 32 + L.nx, rows_smem<S>(L.nx), st>>>(L, a, w);
         return;
     }
     if constexpr (S::shifted && !MACRO) {
@@ -289,7 +291,7 @@ static int rows_occupancy(int nx, bool pairs) {
             return e == cudaSuccess ? n : 0;
         }
     }
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows<S, 0, true, false>, 32 + nx, rows_smem<S>(nx));
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bulk_rows<S, 0, true, false, false>, 32 + nx, rows_smem<S>(nx));
     return e == cudaSuccess ? n : 0;
 }
 
@@ -311,9 +313,12 @@ static cudaError_t prepare_launch() {
         }
     }
     const int rs = (int)rows_smem<S>(ROWS_MAX_NX);
-    for (auto fn : {k_bulk_rows<S, 0, false, false>, k_bulk_rows<S, 0, true, false>, k_bulk_rows<S, 1, false, false>,
-                    k_bulk_rows<S, 1, true, false>, k_bulk_rows<S, 0, false, true>, k_bulk_rows<S, 0, true, true>,
-                    k_bulk_rows<S, 1, false, true>, k_bulk_rows<S, 1, true, true>}) {
+    for (auto fn : {k_bulk_rows<S, 0, false, false, false>, k_bulk_rows<S, 0, true, false, false>,
+                    k_bulk_rows<S, 1, false, false, false>, k_bulk_rows<S, 1, true, false, false>,
+                    k_bulk_rows<S, 0, false, false, true>, k_bulk_rows<S, 0, true, false, true>,
+                    k_bulk_rows<S, 1, false, false, true>, k_bulk_rows<S, 1, true, false, true>,
+                    k_bulk_rows<S, 0, false, true, true>, k_bulk_rows<S, 0, true, true, true>,
+                    k_bulk_rows<S, 1, false, true, true>, k_bulk_rows<S, 1, true, true, true>}) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, rs);
         if (e != cudaSuccess) return e;
     }

@@ -82,6 +82,7 @@ struct lbmgpu_handle {
     unsigned nblocks = 0;
     double* block_part_b = nullptr;
     unsigned nblocks_b = 0;
+    int* row_claim = nullptr;      // staged-row bulk: row counter, CTAs done
     int* ordermap = nullptr;
     int* chg_node = nullptr;
     int* chg_key = nullptr;
@@ -167,6 +168,17 @@ int bulk_kind() {
     return 0;
 }
 
+// SMs the staged-row bulk leaves free for the zone and squirmer kernels, which
+// run beside it on the second stream: LBMGPU_ROWS_RESERVE, else ROWS_RESERVE
+// with a squirmer and none without one (nothing then runs beside the bulk).
+constexpr int ROWS_RESERVE = 0;
+int rows_reserve(bool squirmer, int sms) {
+    const char* e = std::getenv("LBMGPU_ROWS_RESERVE");
+    int r = squirmer ? ROWS_RESERVE : 0;
+    if (e && *e) r = std::atoi(e);
+    return std::max(0, std::min(r, sms / 2));
+}
+
 // Capacity of the boundary-link list of a lattice with these parameters (the
 // links lie inside the sphere's box, so the box volume bounds them).
 int link_capacity(const lbmgpu_params& p) {
@@ -198,6 +210,7 @@ StreamArgs stream_args(lbmgpu_handle* h, const StepPlan& sp) {
     for (int d = 0; d < 3; ++d) a.zw[d] = h->zw[d];
     a.sq = h->sq;
     a.zslot = sp.zslot; a.do_mass = sp.corr ? 1 : 0; a.apply_corr = sp.apply ? 1 : 0;
+    a.row_claim = h->row_claim;
     return a;
 }
 
@@ -466,7 +479,7 @@ void free_all(lbmgpu_handle* h) {
     drop_graph(h);
     if (h->member) { h->f = nullptr; h->flag = nullptr; }
     void* ptrs[] = {h->f, h->flag, h->rho, h->ux, h->uy, h->uz, h->wallrows, h->links, h->linkslot,
-                    h->link_part, h->block_part, h->block_part_b, h->ordermap, h->chg_node, h->chg_key,
+                    h->link_part, h->block_part, h->block_part_b, h->row_claim, h->ordermap, h->chg_node, h->chg_key,
                     h->cand, h->mark, h->traj, h->sq, h->scratch, h->small, h->shell, h->shell_hdr,
                     h->packed, h->snap};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -747,7 +760,13 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
                 h->geom.rows_n = rows * planes;
                 h->geom.rows_ylo = p->walls_y ? 2 : 0;
                 h->geom.rows_zlo = p->walls_z ? 2 : 0;
-                h->geom.rows_grid = (unsigned)std::min<long long>((long long)sms * per_sm, (long long)rows * planes);
+                h->geom.rows_grid = (unsigned)((long long)sms * per_sm);
+                h->geom.rows_reserve = rows_reserve(h->has_sq != 0, sms);
+                if (const char* e = std::getenv("LBMGPU_ROWS_CAP"); e && std::atoi(e) > 0) {
+                    h->geom.rows_cap = std::atoi(e);
+                    h->geom.rows_grid = (unsigned)std::max<long long>(
+                        h->geom.rows_grid, ((long long)rows * planes + h->geom.rows_cap - 1) / h->geom.rows_cap);
+                }
             }
         }
     }
@@ -792,6 +811,7 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     CTRY(cudaMalloc(&h->scratch, N * sizeof(double)));
     CTRY(cudaMalloc(&h->block_part, (size_t)h->nblocks * BLOCK_PART * sizeof(double)));
     CTRY(cudaMalloc(&h->block_part_b, (size_t)h->nblocks_b * BLOCK_PART * sizeof(double)));
+    CTRY(cudaMalloc(&h->row_claim, 2 * sizeof(int)));
     CTRY(cudaMalloc(&h->wallrows, std::max<size_t>(2, hi.wallrows.size()) * sizeof(int)));
     CTRY(cudaMalloc(&h->sq, sizeof(SqState)));
     CTRY(cudaMalloc(&h->small, (2 * MASS_GRID + 4 * DIAG_GRID + 16) * sizeof(double)));
@@ -817,6 +837,7 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     h->launches += 5;
     CTRY(cudaMemsetAsync(h->block_part, 0, (size_t)h->nblocks * BLOCK_PART * sizeof(double), st));
     CTRY(cudaMemsetAsync(h->block_part_b, 0, (size_t)h->nblocks_b * BLOCK_PART * sizeof(double), st));
+    CTRY(cudaMemsetAsync(h->row_claim, 0, 2 * sizeof(int), st));
     if (!hi.wallrows.empty())
         CTRY(cudaMemcpyAsync(h->wallrows, hi.wallrows.data(), hi.wallrows.size() * sizeof(int),
                              cudaMemcpyHostToDevice, st));

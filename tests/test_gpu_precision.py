@@ -11,12 +11,13 @@ node within R + 3 of the sphere's final centre).
 Bounds (stated per form, from the measured errors with a margin):
   * FP64 vs the reference: relative L2 <= 1e-10 in u and rho on the sample and
     the shell, centre and orientation to 1e-10;
-  * squirmer drift |X_form - X_fp64| / |displacement| <= 1e-4 (the target);
-  * velocity field: see U_BOUND -- the FP32 form holds 1e-5 until the first
-    node changes type one step apart from the FP64 run (a remap decision on
-    r^2 < R^2 flipped by ~1e-6 cells of position difference); after that the
-    difference is the acoustic footprint of those events, bounded here at the
-    value measured on the full run, not at 1e-5.
+  * squirmer drift |X_form - X_fp64| / |displacement| <= 1e-4 (the target;
+    FP32 storage, measured at 3.5e-10 at most, is held to 1e-8);
+  * FP32 storage (FP64 arithmetic): u within 1e-5 of FP64 over the whole field
+    (the target), and within U_BOUND, a margin over the measured 2.5e-8 ..
+    4.0e-8;
+  * FP16 storage (FP32 arithmetic): its 2^-11 resolution of the stored
+    deviation sets the error; U_BOUND is a margin over the measured values.
 """
 import numpy as np
 import pytest
@@ -27,12 +28,14 @@ from lbm_solver_3d_b200.workloads import workload_params
 pytestmark = pytest.mark.gpu
 
 CASES = ("bulk_m3", "bulk_0", "bulk_p3")
-# relative L2 of u and rho over the whole field after 10000 steps, per form:
-# measured 1.1e-4 .. 2.0e-4 (FP32) and 1.6e-4 .. 5.8e-3 (FP16) in u, 1.8e-10 ..
-# 1.4e-9 (FP32) and 1e-9 .. 4.3e-8 (FP16) in rho over beta = -3, 0, +3
-U_BOUND = {"fp32": 5e-4, "fp16": 1.5e-2}
-RHO_BOUND = {"fp32": 1e-8, "fp16": 2e-7}
-DRIFT_BOUND = 1e-4
+# relative L2 of u and rho over the whole field after 10000 steps, per form,
+# measured over beta = -3, 0, +3 on a B200: u 2.5e-8 .. 4.0e-8 (FP32) and
+# 1.6e-4 .. 5.8e-3 (FP16); rho 3.4e-13 .. 2.1e-12 (FP32) and 9.9e-10 .. 4.3e-8
+# (FP16); drift 1.1e-10 .. 3.5e-10 (FP32) and 3.0e-7 .. 5.4e-5 (FP16)
+U_TARGET = {"fp32": 1e-5}
+U_BOUND = {"fp32": 2e-7, "fp16": 1.5e-2}
+RHO_BOUND = {"fp32": 1e-11, "fp16": 2e-7}
+DRIFT_BOUND = {"fp32": 1e-8, "fp16": 1e-4}
 
 
 def rel(a, b, m):
@@ -91,6 +94,8 @@ def test_precision_form_against_fp64_full_length(fp64_runs, case, form):
     nflip = int((flag != f64).sum())
     print(f"{case} {form}: u {eu:.2e} rho {er:.2e} drift {drift:.2e} |dX| {np.abs(sq['X'] - sq64['X']).max():.2e} "
           f"node types differing {nflip}")
-    assert drift <= DRIFT_BOUND
+    assert drift <= DRIFT_BOUND[form]
     assert er <= RHO_BOUND[form]
     assert eu <= U_BOUND[form]
+    if form in U_TARGET:
+        assert eu <= U_TARGET[form]
