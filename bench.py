@@ -270,6 +270,10 @@ def warm_rate(run, warmup, stream):
     return ev0.elapsed_time(ev1) / max(1, warmup - 1)
 
 
+# the bulk kernel of steps without sums, per storage form (nx a multiple of 64)
+BULK_KERNEL = {"fp64": "k_bulk_rows", "fp32": "k_bulk_rows", "fp16": "k_bulk_rows2"}
+
+
 def measure_lattice(p, prec, args, stream, dev, pg=None):
     """MLUPS of K steps and the bulk kernel's roofline for one storage form."""
     from lbm_solver_3d_b200.solver import Solver
@@ -291,7 +295,7 @@ def measure_lattice(p, prec, args, stream, dev, pg=None):
     if tf.exists():
         try:
             tr = json.loads(tf.read_text())
-            traffic = tr.get(f"k_bulk_rows:{args.workload}:{prec}", tr.get(f"k_bulk:{args.workload}:{prec}"))
+            traffic = tr.get(f"{BULK_KERNEL[prec]}:{args.workload}:{prec}")
         except Exception:
             traffic = None
     return {
@@ -299,8 +303,8 @@ def measure_lattice(p, prec, args, stream, dev, pg=None):
         # kernels of the K-step window alone (the span's extra steps excluded)
         "launches": int(round(launches * args.steps / (args.steps + 2 * pre))),
         "clocks": clocks,
-        "roofline": {"bound": "hbm", "kernel": "bulk collide-stream (k_bulk_rows on steps without sums, k_bulk "
-                                               "on the one in ten with sums; averaged)",
+        "roofline": {"bound": "hbm", "kernel": f"bulk collide-stream ({BULK_KERNEL[prec]} on steps without sums, "
+                                               "k_bulk_rows with sums on the one in ten with sums; averaged)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "bytes_per_launch": bytes_per_launch, "launch_ms": kt["bulk"],

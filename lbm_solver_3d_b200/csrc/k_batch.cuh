@@ -390,6 +390,31 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m))
                  : "memory");
 }
+// shared -> global bulk copy (this thread's bulk group); both addresses 16-byte
+// aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// this thread's bulk groups have finished reading their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and have completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// this thread's shared-memory writes become visible to later bulk copies
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// named barrier `id` over `n` threads (a multiple of 32) that also returns the
+// AND of p over them: the same value in every participating thread
+__device__ __forceinline__ bool bar_and(int id, int n, bool p) {
+    unsigned r;
+    asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
+                 "bar.red.and.pred po, %2, %3, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
+                 : "=r"(r) : "r"((unsigned)p), "r"(id), "r"(n) : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void bar_sync_n(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
 // 16-byte aligned start and rounded-up length of the copy of [p, p + bytes)
 __device__ __forceinline__ void span16(const void* p, size_t bytes, uintptr_t& start, unsigned& len, int& off) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -816,10 +841,8 @@ __global__ void __launch_bounds__(RUNS_THREADS, 2) k_bulk_runs(const Lattice* __
 //  ROWS_MAX_NX), persistent over the interior rows (y = ylo + r % nry,
 //  z = zlo + r / nry), which the producers claim one at a time from a counter
 //  (RowsWork): a CTA that starts late, or shares its SM with other kernels,
-//  takes fewer rows instead of ending late. CTAs that find themselves on one
-//  of the `reserve` SMs with the lowest %smid leave at once, so the zone and
-//  squirmer kernels of the second stream always find whole SMs free while
-//  this grid runs (a grid that held every SM would put them after it).
+//  takes fewer rows instead of ending late. CTAs that land on one of the
+//  `reserve` lowest-numbered SMs leave at once (rows_idle).
 //    producer   per row: claims the row, waits for the stage to be free
 //               (empty barrier), publishes the row number, then
 //               lane i < 19 copies direction-row i of the state -- A[i] of row
@@ -854,7 +877,6 @@ __host__ __device__ constexpr size_t rows_stage_bytes(int nx) {
 struct RowsWork {
     int nry, nrows, ylo, zlo;   // rows nry x (nrows / nry) from (ylo, zlo)
     int reserve;                // CTAs on SMs with %smid < reserve take no rows
-    int cap;                    // rows one CTA takes at most (0: no limit)
     int* claim;
 };
 
@@ -862,6 +884,15 @@ __device__ __forceinline__ unsigned sm_id() {
     unsigned r;
     asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
     return r;
+}
+
+// A CTA on one of the reserved SMs takes no rows, so that the squirmer update
+// (one CTA of 512 threads, which needs an SM to itself) finds one free while
+// the persistent grid runs -- except the grid's last CTA, so that the rows are
+// done whatever the placement (the claim counter lets one CTA finish them
+// all). Uniform over the CTA.
+__device__ __forceinline__ bool rows_idle(const RowsWork& w) {
+    return (int)sm_id() < w.reserve && blockIdx.x + 1 < gridDim.x;
 }
 
 // Populations of node x from a staged row (whole direction-rows of nx elements;
@@ -909,15 +940,6 @@ __device__ __forceinline__ void stage_row(const Lattice& L, const StreamArgs& a,
     }
 }
 
-// A CTA on a reserved SM takes no rows, and any other takes at most w.cap --
-// except the grid's last CTA, which takes whatever is left, so that every row
-// is done whatever the grid's placement (the claim counter lets one CTA finish
-// them all). Uniform over the CTA.
-__device__ __forceinline__ bool rows_idle(const RowsWork& w) {
-    return (int)sm_id() < w.reserve && blockIdx.x + 1 < gridDim.x;
-}
-__device__ __forceinline__ int rows_cap(const RowsWork& w) { return blockIdx.x + 1 < gridDim.x ? w.cap : 0; }
-
 // The producer loop shared by k_bulk_rows and k_bulk_rows2 (warp 0): claim a
 // row, wait for its stage, publish it in rowid[q] and stage it; -1 ends the
 // consumers' loop. Returns with s_issued = stages armed with copies.
@@ -925,11 +947,10 @@ template <class S, int PAR, int NST>
 __device__ __forceinline__ void rows_produce(const Lattice& L, const StreamArgs& a, const RowsWork& w,
                                              unsigned char* raw, size_t stage, uint64_t* full, uint64_t* empty,
                                              int* rowid, volatile int& s_abort, int& s_issued, int lane) {
-    const int cap = rows_cap(w);
     for (int k = 0;; ++k) {
         const int q = k % NST;
-        int r = w.nrows;
-        if (lane == 0 && (cap == 0 || k < cap)) r = atomicAdd(w.claim, 1);   // before the wait: its latency overlaps it
+        int r = 0;
+        if (lane == 0) r = atomicAdd(w.claim, 1);   // before the wait: its latency overlaps it
         r = __shfl_sync(0xffffffffu, r, 0);
         if (k >= NST) {
             int go = 1;
@@ -1008,7 +1029,6 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = L.nx, nupd = nx >> 5;
     const size_t stage = rows_stage_bytes<S>(nx);
-    const bool idle = rows_idle(w);
     if (tid == 0) {
         for (int q = 0; q < NST; ++q) {
             mbar_init(&full[q], 1);
@@ -1022,7 +1042,7 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
     }
     __syncthreads();
 
-    if (idle) {
+    if (rows_idle(w)) {
     } else if (warp == 0) {
         rows_produce<S, PAR, NST>(L, a, w, rows_raw, stage, full, empty, rowid, s_abort, s_issued, lane);
     } else {
@@ -1084,9 +1104,22 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX, RowsCfg<S>::MINB) k_bulk_row
 //  thread (nx a multiple of 64), for the FP16 form, whose one-node kernel is
 //  bound by instruction issue rather than memory: the directions without an x
 //  shift are read from the stage as one 4-byte pair, and the results leave
-//  through pair_collide_store (paired conversions and 4-byte stores, the
-//  x-shifted directions exchanged between lanes), the second half of
-//  k_bulk_pair. Same staging, barriers, bounded waits and drain as k_bulk_rows.
+//  through one of two paths, chosen per row by a vote of the update warps:
+//    whole row  every node of the row is updated here (no zone, solid or
+//               wall node): each direction's results form one whole row of
+//               the next state (even step: A[opp(i)] of row (y, z) at x; odd
+//               step: A[i] of row (y + c_iy, z + c_iz) at x + c_ix, wrapped),
+//               so they are written over the stage (every read of it is done
+//               by then) and leave as 19 bulk copies shared -> global, issued
+//               by the first update warp, which releases the stage once the
+//               copies have read it;
+//    otherwise  pair_collide_store (paired conversions and 4-byte stores, the
+//               x-shifted directions exchanged between lanes), the second
+//               half of k_bulk_pair.
+//  The update warps meet at named barrier 1 (a timed-out wait or an abort is
+//  folded into the barrier's AND, so they leave the loop together and none
+//  waits for a warp that has left). Same staging, claiming, bounded waits and
+//  drain as k_bulk_rows.
 // ---------------------------------------------------------------------------
 template <class S> struct Rows2Cfg;
 template <> struct Rows2Cfg<StoreF16> { static constexpr int NST = 5, MINB = 4; };
@@ -1107,7 +1140,6 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = L.nx, nupd = nx >> 6;
     const size_t stage = rows_stage_bytes<S>(nx);
-    const bool idle = rows_idle(w);
     if (tid == 0) {
         for (int q = 0; q < NST; ++q) {
             mbar_init(&full[q], 1);
@@ -1120,19 +1152,28 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
     }
     __syncthreads();
 
-    if (idle) {
+    if (rows_idle(w)) {
     } else if (warp == 0) {
         rows_produce<S, PAR, NST>(L, a, w, rows_raw, stage, full, empty, rowid, s_abort, s_issued, lane);
     } else {
         // ---------------- update threads: nodes x0 = 2 t, x0 + 1 ----------------
         T* __restrict__ fw = static_cast<T*>(a.f);
-        const int x0 = 2 * (tid - 32);
+        const int x0 = 2 * (tid - 32), nthr = nupd * 32;
+        bool stored = false;   // this thread issued bulk stores (waits for them before it exits)
         for (int k = 0;; ++k) {
-            const int r = rows_next<NST>(a, full, rowid, s_abort, k, lane);
-            if (r < 0) break;
             const int q = k % NST;
+            bool ok = mbar_wait(&full[q], (uint32_t)((k / NST) & 1));
+            ok = __all_sync(0xffffffffu, ok);
+            // one verdict for all update warps (named barrier 1): no warp may
+            // leave the loop while another waits at that barrier
+            if (!bar_and(1, nthr, ok && !s_abort)) {
+                if (lane == 0 && !ok && !s_abort) { s_abort = 1; atomicOr(&a.sq->status, ST_WATCHDOG); }
+                break;
+            }
+            const int r = rowid[q];
+            if (r < 0) break;   // the same stage entry for every warp
             const int y = w.ylo + r % w.nry, z = w.zlo + r / w.nry;
-            const T* sb = reinterpret_cast<const T*>(rows_raw + (size_t)q * stage);
+            T* sb = reinterpret_cast<T*>(rows_raw + (size_t)q * stage);
             const uint8_t* sf = rows_raw + (size_t)q * stage + (size_t)Q * nx * sizeof(T);
             bool act0 = (sf[x0] & (uint8_t)~NEAR_WALL) == 0, act1 = (sf[x0 + 1] & (uint8_t)~NEAR_WALL) == 0;
             if (SQ && in_zone_axis(y, zb.lo[1], zb.w[1], L.ny, L.walls_y) &&
@@ -1140,7 +1181,6 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
                 act0 = act0 && !in_zone_axis(x0, zb.lo[0], zb.w[0], nx, false);
                 act1 = act1 && !in_zone_axis(x0 + 1, zb.lo[0], zb.w[0], nx, false);
             }
-            const PairRow pr(L, x0, y, z, lane, act0, act1);
             float d0[Q], d1[Q];
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
@@ -1156,11 +1196,51 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
                     d1[i] = S::ld(rowi + (x0 + 2 == nx ? 0 : x0 + 2));
                 }
             }
-            if (L.force_free) pair_collide_store<S, PAR, false>(L, a, fw, pr, d0, d1);
-            else pair_collide_store<S, PAR, true>(L, a, fw, pr, d0, d1);
+            // every read of the stage is done; is every node of the row updated here?
+            if (bar_and(1, nthr, act0 && act1)) {
+                // Whole row: each direction's results form one whole row of the
+                // next state (even step: A[opp(i)] of row (y, z) at x; odd step:
+                // A[i] of row (y + c_iy, z + c_iz) at x + c_ix, wrapped), so they
+                // are written over the stage and leave as 19 bulk copies.
+                auto put = [&](int i, float v0, float v1) {
+                    if (PAR == 0) {
+                        S::st2(sb + OPP(i) * nx + x0, v0, v1);
+                    } else if (CX(i) == 0) {
+                        S::st2(sb + i * nx + x0, v0, v1);
+                    } else if (CX(i) > 0) {
+                        S::st(sb + i * nx + x0 + 1, v0);
+                        S::st(sb + i * nx + (x0 + 2 == nx ? 0 : x0 + 2), v1);
+                    } else {
+                        S::st(sb + i * nx + (x0 == 0 ? nx - 1 : x0 - 1), v0);
+                        S::st(sb + i * nx + x0, v1);
+                    }
+                };
+                if (L.force_free) pair_collide<S, PAR, false>(L, a, d0, d1, put);
+                else pair_collide<S, PAR, true>(L, a, d0, d1, put);
+                fence_async_smem();
+                bar_sync_n(1, nthr);
+                if (warp == 1 && lane < Q) {
+                    const int i = lane;
+                    int yd = y, zd = z;
+                    if (PAR == 1) {
+                        yd = y + c_cy_rt(i); if (yd < 0) yd += L.ny; else if (yd >= L.ny) yd -= L.ny;
+                        zd = z + c_cz_rt(i); if (zd < 0) zd += L.nz; else if (zd >= L.nz) zd -= L.nz;
+                    }
+                    bulk_s2g(fw + (size_t)i * L.N + (size_t)nx * (yd + (size_t)L.ny * zd), sb + (size_t)i * nx,
+                             (unsigned)(nx * sizeof(T)));
+                    bulk_commit();
+                    bulk_wait_read();   // the stage may be refilled once the copy has read it
+                    stored = true;
+                }
+            } else {
+                const PairRow pr(L, x0, y, z, lane, act0, act1);
+                if (L.force_free) pair_collide_store<S, PAR, false>(L, a, fw, pr, d0, d1);
+                else pair_collide_store<S, PAR, true>(L, a, fw, pr, d0, d1);
+            }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[q]);
         }
+        if (stored) bulk_wait_all();
     }
     rows_finish<NST>(w, full, s_abort, s_issued, tid);
 }

@@ -53,7 +53,14 @@
 
 namespace lbmgpu {
 
-constexpr int BOUNDARY_BLOCK = 128;
+// Threads of a zone CTA, and the registers the single-lattice zone kernel may
+// use. Sized so that a zone CTA fits on an SM beside the staged-row bulk
+// kernel's two CTAs: those are 18 warps of 96 registers, spread 5/5/4/4 over
+// the SM's four 16,384-register partitions, which leaves 4,096 registers in
+// two of them -- one warp of 128 registers each. The zone of the next step
+// then runs while the bulk of this one does instead of after it.
+constexpr int BOUNDARY_BLOCK = 64;
+constexpr int ZONE_MAX_REGS = 128;
 
 // LBM::offsetFromSquirmer (lbm.cpp:100-104): minimum image in x always, in
 // y/z only where there is no wall.
@@ -236,24 +243,61 @@ __device__ __forceinline__ void shifted_moments(const Lattice& L, const float* d
         if (CY(i) > 0) jy += di; else if (CY(i) < 0) jy -= di;
         if (CZ(i) > 0) jz += di; else if (CZ(i) < 0) jz -= di;
     }
-    rho = A(1) + dr * (A)S::INV;
-    const A inv = A(1) / rho;
-    u = (jx * (A)S::INV + A(0.5) * Coll<A>::F(L, 0)) * inv;
-    v = (jy * (A)S::INV + A(0.5) * Coll<A>::F(L, 1)) * inv;
-    wz = (jz * (A)S::INV + A(0.5) * Coll<A>::F(L, 2)) * inv;
+    if constexpr (sizeof(A) == 4) {   // every operation spelled out: no kernel contracts it differently
+        rho = __fmaf_rn(dr, S::INV, 1.0f);
+        const float inv = __fdiv_rn(1.0f, rho);
+        u = __fmul_rn(__fmaf_rn(jx, S::INV, __fmul_rn(0.5f, L.Ff[0])), inv);
+        v = __fmul_rn(__fmaf_rn(jy, S::INV, __fmul_rn(0.5f, L.Ff[1])), inv);
+        wz = __fmul_rn(__fmaf_rn(jz, S::INV, __fmul_rn(0.5f, L.Ff[2])), inv);
+    } else {
+        rho = A(1) + dr * (A)S::INV;
+        const A inv = A(1) / rho;
+        u = (jx * (A)S::INV + A(0.5) * Coll<A>::F(L, 0)) * inv;
+        v = (jy * (A)S::INV + A(0.5) * Coll<A>::F(L, 1)) * inv;
+        wz = (jz * (A)S::INV + A(0.5) * Coll<A>::F(L, 2)) * inv;
+    }
 }
+
+// The per-node terms of the collision: k15 = 1.5 |u|^2, uF = u . F and
+// srho = S::SC * rho (FP32: explicit operations, as in shifted_moments).
+template <class S, class A = typename S::A>
+__device__ __forceinline__ void shifted_terms(const Lattice& L, A rho, A u, A v, A wz, A& k15, A& uF, A& srho) {
+    if constexpr (sizeof(A) == 4) {
+        k15 = __fmul_rn(1.5f, __fmaf_rn(wz, wz, __fmaf_rn(v, v, __fmul_rn(u, u))));
+        uF = __fmaf_rn(wz, L.Ff[2], __fmaf_rn(v, L.Ff[1], __fmul_rn(u, L.Ff[0])));
+        srho = __fmul_rn(S::SC, rho);   // a power of two: exact
+    } else {
+        k15 = A(1.5) * (u * u + v * v + wz * wz);
+        uF = u * Coll<A>::F(L, 0) + v * Coll<A>::F(L, 1) + wz * Coll<A>::F(L, 2);
+        srho = (A)S::SC * rho;
+    }
+}
+
+// weight class of direction i: 0 rest, 1 axes, 2 diagonals
+__host__ __device__ constexpr int wclass(int i) { return i == 0 ? 0 : (i <= 6 ? 1 : 2); }
 
 // TRT + Guo post-collision values in storage units (lbm.cpp:162-172, deviation
 // form), in the form's arithmetic A: the rest population, and one opposite pair
-// (i, i+1) with f+, feq+ and S+ shared and the odd parts of opposite signs.
-// srho = S::SC * rho, k15 = 1.5 |u|^2, uF = u . F. FORCE = false drops the Guo
-// source terms, which vanish for F = 0.
+// (i, i+1). srho = S::SC * rho, k15 = 1.5 |u|^2, uF = u . F. FORCE = false
+// drops the Guo source terms, which vanish for F = 0.
+//
+// f+, feq+ and S+ are shared by the pair and the odd parts have opposite signs.
+// In FP32 arithmetic every operation is an explicit intrinsic (and the
+// constants are formed once on the host), so that every kernel rounds the same
+// way: left to the compiler, a*b + c*d may be contracted into an FMA either way
+// round, and differently in different kernels.
 template <class S, bool FORCE, class A = typename S::A>
 __device__ __forceinline__ A rest_post(const Lattice& L, A d0, A dr, A srho, A k15, A uF) {
     using C = Coll<A>;
-    const A eP = C::w(0) * (dr - srho * k15);
-    return FORCE ? d0 - C::omP(L) * (d0 - eP) - (A)S::SC * C::gP(L) * C::w(0) * A(3) * uF
-                 : d0 - C::omP(L) * (d0 - eP);
+    if constexpr (sizeof(A) == 4) {
+        const float eP = __fmul_rn(C::w(0), __fmaf_rn(-srho, k15, dr));
+        const float o = __fmaf_rn(-L.omPf, __fsub_rn(d0, eP), d0);
+        return FORCE ? __fmaf_rn(-3.0f * S::SC * L.gPw[0], uF, o) : o;
+    } else {
+        const A eP = C::w(0) * (dr - srho * k15);
+        const A o = d0 - C::omP(L) * (d0 - eP);
+        return FORCE ? o - (A)S::SC * C::gP(L) * C::w(0) * A(3) * uF : o;
+    }
 }
 template <class S, bool FORCE, class A = typename S::A>
 __device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, A u, A v, A wz, A dr, A srho, A k15,
@@ -261,19 +305,35 @@ __device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, 
     using C = Coll<A>;
     const A cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
     const A w = C::w(i);
-    const A eP = w * (dr + srho * (A(4.5) * cu * cu - k15));  // feq+ - w, storage units
-    const A eM = A(3) * w * srho * cu;                        // feq-
-    const A fP = A(0.5) * (di + dio), fM = A(0.5) * (di - dio);
-    A a, b;
-    if (FORCE) {
-        a = (A)S::SC * C::gP(L) * w * (A(9) * cu * C::cF(L, i) - A(3) * uF) - C::omP(L) * (fP - eP);
-        b = (A)S::SC * C::cm(L, i) - C::omM(L) * (fM - eM);
+    if constexpr (sizeof(A) == 4) {
+        // every operation spelled out, so that no kernel contracts it differently
+        const int c = wclass(i);
+        const float eP = __fmul_rn(C::w(i), __fmaf_rn(srho, __fmaf_rn(__fmul_rn(4.5f, cu), cu, -k15), dr));
+        const float eM = __fmul_rn(__fmul_rn(3.0f * C::w(i), srho), cu);
+        const float fP = __fmul_rn(0.5f, __fadd_rn(di, dio)), fM = __fmul_rn(0.5f, __fsub_rn(di, dio));
+        float a = __fmul_rn(-L.omPf, __fsub_rn(fP, eP));
+        float b = __fmul_rn(-L.omMf, __fsub_rn(fM, eM));
+        if (FORCE) {
+            a = __fmaf_rn(S::SC * L.gPw[c], __fmaf_rn(__fmul_rn(9.0f, cu), L.cF[i], __fmul_rn(-3.0f, uF)), a);
+            b = __fadd_rn(b, S::SC * L.cm[i]);
+        }
+        oi = __fadd_rn(__fadd_rn(di, a), b);
+        oo = __fsub_rn(__fadd_rn(dio, a), b);
     } else {
-        a = -C::omP(L) * (fP - eP);
-        b = -C::omM(L) * (fM - eM);
+        const A eP = w * (dr + srho * (A(4.5) * cu * cu - k15));   // feq+ - w, storage units
+        const A eM = A(3) * w * srho * cu;                          // feq-
+        const A fP = A(0.5) * (di + dio), fM = A(0.5) * (di - dio);
+        A a, b;
+        if (FORCE) {
+            a = (A)S::SC * C::gP(L) * w * (A(9) * cu * C::cF(L, i) - A(3) * uF) - C::omP(L) * (fP - eP);
+            b = (A)S::SC * C::cm(L, i) - C::omM(L) * (fM - eM);
+        } else {
+            a = -C::omP(L) * (fP - eP);
+            b = -C::omM(L) * (fM - eM);
+        }
+        oi = di + a + b;
+        oo = dio + a - b;
     }
-    oi = di + a + b;
-    oo = dio + a - b;
 }
 
 // Collide and push of a node with only fluid neighbours, in the form's
@@ -503,10 +563,8 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         if (GENERAL) out.rho = (double)rho;
         if (store_rho) a.rho[n] = 1.0 + (double)dr * S::INV;
         if (MACRO) { a.ux[n] = u; a.uy[n] = v; a.uz[n] = wz; }
-        const AR usq = u * u + v * v + wz * wz;
-        const AR uF = u * Coll<AR>::F(L, 0) + v * Coll<AR>::F(L, 1) + wz * Coll<AR>::F(L, 2);
-        const AR k15 = AR(1.5) * usq;
-        const AR srho = (AR)S::SC * rho;
+        AR k15, uF, srho;
+        shifted_terms<S>(L, rho, u, v, wz, k15, uF, srho);
         if (!boundary) {
             if (L.force_free)   // uniform: the Guo source terms are exactly zero
                 plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
@@ -685,15 +743,11 @@ struct PairRow {
     }
 };
 
-// Collide and store of a thread's two nodes (the second half of k_bulk_pair,
-// shared with the staged two-node kernel): d0, d1 are the 19 logical stored
-// numbers of x0 and x0 + 1. Every lane of the warp calls it (the stores
-// shuffle the x-shifted values between lanes).
-template <class S, int PAR, bool FORCE>
-__device__ __forceinline__ void pair_collide_store(const Lattice& L, const StreamArgs& a, typename S::T* __restrict__ f,
-                                                   const PairRow& pr, float* d0, float* d1) {
-    using T = typename S::T;
-    const unsigned N = L.N;
+// Collision of a thread's two nodes x0, x0 + 1 from their 19 logical stored
+// numbers d0, d1; put(i, a0, a1) receives the post-collision values of
+// direction i of both nodes, rounded to the FP32 they are stored through.
+template <class S, int PAR, bool FORCE, class Put>
+__device__ __forceinline__ void pair_collide(const Lattice& L, const StreamArgs& a, float* d0, float* d1, Put&& put) {
     if (a.apply_corr) {
         const double corr = a.sq->corr_d;
 #pragma unroll
@@ -703,15 +757,35 @@ __device__ __forceinline__ void pair_collide_store(const Lattice& L, const Strea
         }
     }
     using AR = typename S::A;
-    using C = Coll<AR>;
     AR dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
     shifted_moments<S>(L, d0, dr0, rho0, u0, v0, w0);
     shifted_moments<S>(L, d1, dr1, rho1, u1, v1, w1);
-    const AR q0 = u0 * u0 + v0 * v0 + w0 * w0, q1 = u1 * u1 + v1 * v1 + w1 * w1;
-    const AR k0 = AR(1.5) * q0, k1 = AR(1.5) * q1;
-    const AR uF0 = u0 * C::F(L, 0) + v0 * C::F(L, 1) + w0 * C::F(L, 2);
-    const AR uF1 = u1 * C::F(L, 0) + v1 * C::F(L, 1) + w1 * C::F(L, 2);
-    const AR sr0 = (AR)S::SC * rho0, sr1 = (AR)S::SC * rho1;
+    AR k0, k1, uF0, uF1, sr0, sr1;
+    shifted_terms<S>(L, rho0, u0, v0, w0, k0, uF0, sr0);
+    shifted_terms<S>(L, rho1, u1, v1, w1, k1, uF1, sr1);
+    put(0, (float)rest_post<S, FORCE>(L, (AR)d0[0], dr0, sr0, k0, uF0),
+        (float)rest_post<S, FORCE>(L, (AR)d1[0], dr1, sr1, k1, uF1));
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+        AR a0i, a0o, a1i, a1o;
+        pair_post<S, FORCE>(L, i, (AR)d0[i], (AR)d0[i + 1], u0, v0, w0, dr0, sr0, k0, uF0, a0i, a0o);
+        pair_post<S, FORCE>(L, i, (AR)d1[i], (AR)d1[i + 1], u1, v1, w1, dr1, sr1, k1, uF1, a1i, a1o);
+        // direction i's post value goes where the next state reads logical
+        // f_i: even step -> A[opp(i)][n]; odd step -> A[i][n + c_i]
+        put(i, (float)a0i, (float)a1i);
+        put(i + 1, (float)a0o, (float)a1o);
+    }
+}
+
+// Collide and store of a thread's two nodes (the second half of k_bulk_pair,
+// shared with the staged two-node kernel): d0, d1 are the 19 logical stored
+// numbers of x0 and x0 + 1. Every lane of the warp calls it (the stores
+// shuffle the x-shifted values between lanes).
+template <class S, int PAR, bool FORCE>
+__device__ __forceinline__ void pair_collide_store(const Lattice& L, const StreamArgs& a, typename S::T* __restrict__ f,
+                                                   const PairRow& pr, float* d0, float* d1) {
+    using T = typename S::T;
+    const unsigned N = L.N;
     const int x0 = pr.x0;
     const bool act0 = pr.act0, act1 = pr.act1;
 
@@ -740,18 +814,7 @@ __device__ __forceinline__ void pair_collide_store(const Lattice& L, const Strea
             if (!pr.has_prev && act0) S::st(rowp + pr.xm, a0);
         }
     };
-    put(0, (float)rest_post<S, FORCE>(L, (AR)d0[0], dr0, sr0, k0, uF0),
-        (float)rest_post<S, FORCE>(L, (AR)d1[0], dr1, sr1, k1, uF1));
-#pragma unroll
-    for (int i = 1; i < Q; i += 2) {
-        AR a0i, a0o, a1i, a1o;
-        pair_post<S, FORCE>(L, i, (AR)d0[i], (AR)d0[i + 1], u0, v0, w0, dr0, sr0, k0, uF0, a0i, a0o);
-        pair_post<S, FORCE>(L, i, (AR)d1[i], (AR)d1[i + 1], u1, v1, w1, dr1, sr1, k1, uF1, a1i, a1o);
-        // direction i's post value goes where the next state reads logical
-        // f_i: even step -> A[opp(i)][n]; odd step -> A[i][n + c_i]
-        put(i, (float)a0i, (float)a1i);
-        put(i + 1, (float)a0o, (float)a1o);
-    }
+    pair_collide<S, PAR, FORCE>(L, a, d0, d1, put);
 }
 
 template <class S, int PAR, bool SQ, bool FORCE>
@@ -898,15 +961,16 @@ __device__ __forceinline__ void zone_cell(const Lattice& L, const StreamArgs& a,
     }
 }
 
-// The squirmer state, one word per thread, into a block's shared copy.
+// The squirmer state, word by word, into a block's shared copy.
 __device__ __forceinline__ void copy_sq_state(SqState* dst, const SqState* src) {
     constexpr int NS = (int)(sizeof(SqState) / 4);
-    static_assert(sizeof(SqState) % 4 == 0 && NS <= BOUNDARY_BLOCK, "one word per thread");
-    if ((int)threadIdx.x < NS) reinterpret_cast<uint32_t*>(dst)[threadIdx.x] = reinterpret_cast<const uint32_t*>(src)[threadIdx.x];
+    static_assert(sizeof(SqState) % 4 == 0, "whole words");
+    for (int k = (int)threadIdx.x; k < NS; k += (int)blockDim.x)
+        reinterpret_cast<uint32_t*>(dst)[k] = reinterpret_cast<const uint32_t*>(src)[k];
 }
 
 template <class S, int PAR, bool SQ, bool MACRO>
-__global__ void __launch_bounds__(BOUNDARY_BLOCK) k_zone(const Lattice L, const StreamArgs a) {
+__global__ void __maxnreg__(ZONE_MAX_REGS) k_zone(const Lattice L, const StreamArgs a) {
     pdl_wait();
     pdl_launch_dependents();
     __shared__ __align__(16) SqState zsq;

@@ -26,8 +26,7 @@ struct StreamGeom {
     unsigned rows_grid = 0;
     int rows_nry = 0, rows_n = 0, rows_ylo = 0, rows_zlo = 0;
     bool rows_pairs = false;   // two nodes per update thread (k_bulk_rows2)
-    int rows_reserve = 0;      // SMs (lowest %smid) the rows grid leaves to the second stream
-    int rows_cap = 0;          // rows per CTA at most (0: persistent, no limit)
+    int rows_reserve = 0;      // SMs (lowest %smid) the rows grid leaves to the squirmer update
 };
 
 struct SqArgs;

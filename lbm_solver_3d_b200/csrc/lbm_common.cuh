@@ -111,6 +111,9 @@ struct Lattice {
     // FP32 copies and per-direction forcing constants of the shifted forms:
     // cF[i] = c_i . F and cm[i] = gM * 3 w_i (c_i . F) for the odd i of each pair
     float omPf, omMf, gPf, gMf, Ff[3], uFh[3];
+    // gP w per weight class (0: rest, 1: axes, 2: diagonals), formed once here
+    // so that every kernel's FP32 Guo term rounds the same way
+    float gPw[3];
     float cF[Q], cm[Q];
     int force_free;        // F = 0: the Guo source terms vanish (FP32 arithmetic skips them)
 };

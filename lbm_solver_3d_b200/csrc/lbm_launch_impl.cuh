@@ -11,6 +11,11 @@
 
 namespace lbmgpu {
 
+template <class F>
+static cudaError_t max_shared_split(F* fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+}
+
 template <class S>
 static size_t rows_smem(int nx) { return (size_t)RowsCfg<S>::NST * rows_stage_bytes<S>(nx); }
 template <class S>
@@ -22,7 +27,7 @@ static size_t rows2_smem(int nx) {
 template <class S, int PAR, bool SQ, bool MACRO>
 static void bulk_one(const Lattice& L, const StreamArgs& a, const StreamGeom& g, cudaStream_t st) {
     if (g.rows_grid) {   // rows staged in shared memory (every step; sums in k_bulk's order)
-        const RowsWork w{g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo, g.rows_reserve, g.rows_cap, a.row_claim};
+        const RowsWork w{g.rows_nry, g.rows_n, g.rows_ylo, g.rows_zlo, g.rows_reserve, a.row_claim};
         if constexpr (S::shifted && !MACRO) {
             if (g.rows_pairs && !a.do_mass) {   // no sums this step: two nodes per update thread
                 k_bulk_rows2<S, PAR, SQ><<<g.rows_grid, 32 + L.nx / 2, rows2_smem<S>(L.nx), st>>>(L, a, w);
@@ -323,6 +328,41 @@ static cudaError_t prepare_launch() {
         if (e != cudaSuccess) return e;
     }
     e = cudaFuncSetAttribute(k_squirmer_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)squirmer_smem());
+    if (e != cudaSuccess) return e;
+    // The staged-row bulk and the kernels of the second stream that should run
+    // beside it (zone, squirmer update, wall rows) ask for the largest shared
+    // memory split. Left to the default, two bulk CTAs (2 x 77 KB) get the
+    // 164 KB split, whose 7 KB left over holds no zone CTA (11 KB), and the
+    // zone of the next step then waits for the bulk to end.
+    for (auto fn : {k_bulk_rows<S, 0, false, false, false>, k_bulk_rows<S, 0, true, false, false>,
+                    k_bulk_rows<S, 1, false, false, false>, k_bulk_rows<S, 1, true, false, false>,
+                    k_bulk_rows<S, 0, false, false, true>, k_bulk_rows<S, 0, true, false, true>,
+                    k_bulk_rows<S, 1, false, false, true>, k_bulk_rows<S, 1, true, false, true>,
+                    k_bulk_rows<S, 0, false, true, true>, k_bulk_rows<S, 0, true, true, true>,
+                    k_bulk_rows<S, 1, false, true, true>, k_bulk_rows<S, 1, true, true, true>}) {
+        e = max_shared_split(fn);
+        if (e != cudaSuccess) return e;
+    }
+    if constexpr (S::shifted) {
+        for (auto fn : {k_bulk_rows2<S, 0, false>, k_bulk_rows2<S, 0, true>, k_bulk_rows2<S, 1, false>,
+                        k_bulk_rows2<S, 1, true>}) {
+            e = max_shared_split(fn);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    for (auto fn : {k_zone<S, 0, false, false>, k_zone<S, 0, false, true>, k_zone<S, 0, true, false>,
+                    k_zone<S, 0, true, true>, k_zone<S, 1, false, false>, k_zone<S, 1, false, true>,
+                    k_zone<S, 1, true, false>, k_zone<S, 1, true, true>}) {
+        e = max_shared_split(fn);
+        if (e != cudaSuccess) return e;
+    }
+    for (auto fn : {k_bulk<S, 0, false, false, true>, k_bulk<S, 0, false, true, true>, k_bulk<S, 0, true, false, true>,
+                    k_bulk<S, 0, true, true, true>, k_bulk<S, 1, false, false, true>, k_bulk<S, 1, false, true, true>,
+                    k_bulk<S, 1, true, false, true>, k_bulk<S, 1, true, true, true>}) {
+        e = max_shared_split(fn);
+        if (e != cudaSuccess) return e;
+    }
+    e = max_shared_split(k_squirmer<S>);
     if (e != cudaSuccess) return e;
     cudaError_t es[8] = {staged_attr<S, 0, false, 3>(), staged_attr<S, 0, false, 4>(), staged_attr<S, 0, true, 3>(),
                          staged_attr<S, 0, true, 4>(),  staged_attr<S, 1, false, 3>(), staged_attr<S, 1, false, 4>(),

@@ -168,10 +168,11 @@ int bulk_kind() {
     return 0;
 }
 
-// SMs the staged-row bulk leaves free for the zone and squirmer kernels, which
-// run beside it on the second stream: LBMGPU_ROWS_RESERVE, else ROWS_RESERVE
-// with a squirmer and none without one (nothing then runs beside the bulk).
-constexpr int ROWS_RESERVE = 0;
+// SMs the persistent staged-row bulk leaves to the squirmer update of the
+// second stream, whose CTA needs an SM to itself (a zone CTA fits beside the
+// bulk's CTAs on any SM): LBMGPU_ROWS_RESERVE, else ROWS_RESERVE with a
+// squirmer and none without one.
+constexpr int ROWS_RESERVE = 2;
 int rows_reserve(bool squirmer, int sms) {
     const char* e = std::getenv("LBMGPU_ROWS_RESERVE");
     int r = squirmer ? ROWS_RESERVE : 0;
@@ -707,6 +708,7 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     L.gM = 1.0 - 0.5 * L.omM;
     L.F[0] = p->fx; L.F[1] = p->fy; L.F[2] = p->fz;
     L.omPf = (float)L.omP; L.omMf = (float)L.omM; L.gPf = (float)L.gP; L.gMf = (float)L.gM;
+    for (int c = 0; c < 3; ++c) L.gPw[c] = (float)(L.gP * (c == 0 ? WD(0) : (c == 1 ? WD(1) : WD(7))));
     for (int d = 0; d < 3; ++d) { L.Ff[d] = (float)L.F[d]; L.uFh[d] = 0.0f; }
     L.force_free = L.F[0] == 0.0 && L.F[1] == 0.0 && L.F[2] == 0.0;
     for (int i = 0; i < Q; ++i) {
@@ -760,13 +762,8 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
                 h->geom.rows_n = rows * planes;
                 h->geom.rows_ylo = p->walls_y ? 2 : 0;
                 h->geom.rows_zlo = p->walls_z ? 2 : 0;
-                h->geom.rows_grid = (unsigned)((long long)sms * per_sm);
+                h->geom.rows_grid = (unsigned)std::min<long long>((long long)sms * per_sm, (long long)rows * planes);
                 h->geom.rows_reserve = rows_reserve(h->has_sq != 0, sms);
-                if (const char* e = std::getenv("LBMGPU_ROWS_CAP"); e && std::atoi(e) > 0) {
-                    h->geom.rows_cap = std::atoi(e);
-                    h->geom.rows_grid = (unsigned)std::max<long long>(
-                        h->geom.rows_grid, ((long long)rows * planes + h->geom.rows_cap - 1) / h->geom.rows_cap);
-                }
             }
         }
     }

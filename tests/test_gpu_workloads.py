@@ -87,6 +87,13 @@ def test_squirmer_workload_fp64(Solver, name):
     fl, rho, u, fluid = sampled(s, g)
     assert rel_l2(rho[fluid], g["sample_rho"][fluid]) < 1e-10
     assert rel_l2(u[fluid], g["sample_u"][fluid]) < 1e-10
+    if "shell_idx" in g.files:   # every node within R + 3 of the final centre
+        flag, rho_all, u_all = s.fields()
+        idx = g["shell_idx"]
+        assert np.array_equal(flag.reshape(-1)[idx], g["shell_flag"])
+        sh = g["shell_flag"] == 0
+        assert rel_l2(rho_all.reshape(-1)[idx][sh], g["shell_rho"][sh]) < 1e-10
+        assert rel_l2(u_all.reshape(-1, 3)[idx][sh], g["shell_u"][sh]) < 1e-10
 
 
 @pytest.mark.parametrize("name", ["slit", "bulk_0"])
