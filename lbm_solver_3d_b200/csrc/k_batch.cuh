@@ -390,6 +390,25 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m))
                  : "memory");
 }
+// An L2 policy that evicts first: for the bulk's own traffic, read once per
+// step, so that it does not displace the zone's and the squirmer update's data.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// global -> shared bulk copy with an L2 policy
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, uint64_t* m, uint64_t pol) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)), "l"(pol)
+                 : "memory");
+}
+// shared -> global bulk copy with an L2 policy (this thread's bulk group)
+__device__ __forceinline__ void bulk_s2g_hint(void* dst, const void* src, unsigned bytes, uint64_t pol) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;"
+                 ::"l"(dst), "r"(smem_u32(src)), "r"(bytes), "l"(pol)
+                 : "memory");
+}
 // shared -> global bulk copy (this thread's bulk group); both addresses 16-byte
 // aligned, bytes a multiple of 16
 __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
@@ -933,8 +952,8 @@ __device__ __forceinline__ void stage_row(const Lattice& L, const StreamArgs& a,
             zs = z - c_cz_rt(i); if (zs < 0) zs += L.nz; else if (zs >= L.nz) zs -= L.nz;
         }
         const T* f = static_cast<const T*>(a.f);
-        bulk_g2s(sb + (size_t)i * nx * sizeof(T), f + (size_t)arr * L.N + (size_t)nx * (ys + (size_t)L.ny * zs),
-                 (unsigned)(nx * sizeof(T)), full);
+        bulk_g2s_hint(sb + (size_t)i * nx * sizeof(T), f + (size_t)arr * L.N + (size_t)nx * (ys + (size_t)L.ny * zs),
+                      (unsigned)(nx * sizeof(T)), full, l2_evict_first());
     } else if (lane == Q) {
         bulk_g2s(sb + (size_t)Q * nx * sizeof(T), a.flag + (size_t)nx * (y + (size_t)L.ny * z), (unsigned)nx, full);
     }
@@ -1226,8 +1245,8 @@ __global__ void __launch_bounds__(32 + ROWS_MAX_NX / 2, Rows2Cfg<S>::MINB) k_bul
                         yd = y + c_cy_rt(i); if (yd < 0) yd += L.ny; else if (yd >= L.ny) yd -= L.ny;
                         zd = z + c_cz_rt(i); if (zd < 0) zd += L.nz; else if (zd >= L.nz) zd -= L.nz;
                     }
-                    bulk_s2g(fw + (size_t)i * L.N + (size_t)nx * (yd + (size_t)L.ny * zd), sb + (size_t)i * nx,
-                             (unsigned)(nx * sizeof(T)));
+                    bulk_s2g_hint(fw + (size_t)i * L.N + (size_t)nx * (yd + (size_t)L.ny * zd), sb + (size_t)i * nx,
+                                  (unsigned)(nx * sizeof(T)), l2_evict_first());
                     bulk_commit();
                     bulk_wait_read();   // the stage may be refilled once the copy has read it
                     stored = true;

@@ -336,16 +336,24 @@ __device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, 
     }
 }
 
+template <class S, bool STREAM, class V>
+__device__ __forceinline__ void put_st(typename S::T* p, V v) {
+    if constexpr (STREAM) S::st_cs(p, v);
+    else S::st(p, v);
+}
+
 // Collide and push of a node with only fluid neighbours, in the form's
 // arithmetic on its stored numbers: the rest population, then one opposite
 // pair at a time; each value is rounded to the storage type once, as stored.
-template <class S, int PAR, bool FORCE, class A = typename S::A>
+// STREAM: streaming stores (the bulk's nodes, read again only next step, so
+// they need not displace the zone's and the squirmer update's data in L2).
+template <class S, int PAR, bool FORCE, bool STREAM = false, class A = typename S::A>
 __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
                                             const Nbr& nb, const float* d, A dr, A srho, A u, A v, A wz, A uF, A k15,
                                             bool do_mass, NodeSums& out) {
     {   // rest population: c = 0
         const float o0 = (float)rest_post<S, FORCE>(L, (A)d[0], dr, srho, k15, uF);
-        S::st(f + n, o0);
+        put_st<S, STREAM>(f + n, o0);
         if (do_mass) out.mass += (double)S::rt(o0) * S::INV;
     }
 #pragma unroll
@@ -355,11 +363,11 @@ __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __r
         pair_post<S, FORCE>(L, i, (A)d[i], (A)d[io], u, v, wz, dr, srho, k15, uF, ai, ao);
         const float oi = (float)ai, oo = (float)ao;
         if (PAR == 0) {
-            S::st(f + (size_t)io * N + n, oi);
-            S::st(f + (size_t)i * N + n, oo);
+            put_st<S, STREAM>(f + (size_t)io * N + n, oi);
+            put_st<S, STREAM>(f + (size_t)i * N + n, oo);
         } else {
-            S::st(f + (size_t)i * N + nb.of(n, i), oi);
-            S::st(f + (size_t)io * N + nb.of(n, io), oo);
+            put_st<S, STREAM>(f + (size_t)i * N + nb.of(n, i), oi);
+            put_st<S, STREAM>(f + (size_t)io * N + nb.of(n, io), oo);
         }
         if (do_mass) out.mass += (double)S::rt(oi) * S::INV + (double)S::rt(oo) * S::INV;
     }
@@ -376,7 +384,7 @@ __device__ __forceinline__ void plain_pairs(const Lattice& L, typename S::T* __r
 // terms in the reference's order. The results are the reference's bits
 // (where a term is +-0 its sign may differ, which leaves a nonzero sum as it
 // is). FORCE = false drops the Guo terms: for F = 0 they are +-0.
-template <class S, int PAR, bool FORCE>
+template <class S, int PAR, bool FORCE, bool STREAM = false>
 __device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T* __restrict__ f, unsigned N, unsigned n,
                                                  const Nbr& nb, const double* fv, double r, double u, double v,
                                                  double wz, double usq, double uF, bool do_mass, NodeSums& out) {
@@ -390,7 +398,7 @@ __device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T
         const double SP = WD(0) * (9.0 * cu * cF - 3.0 * uF), SM = WD(0) * 3.0 * cF;
         const double fpost = FORCE ? fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM) + L.gP * SP + L.gM * SM
                                    : fv[0] - L.omP * (fP - feqP) - L.omM * (fM - feqM);
-        S::st(f + n, fpost);
+        put_st<S, STREAM>(f + n, fpost);
         if (do_mass) out.mass += fpost;
     }
 #pragma unroll
@@ -413,11 +421,11 @@ __device__ __forceinline__ void plain_pairs_fp64(const Lattice& L, typename S::T
             fo = fv[io] - A + B;
         }
         if (PAR == 0) {
-            S::st(f + (size_t)io * N + n, fi);
-            S::st(f + (size_t)i * N + n, fo);
+            put_st<S, STREAM>(f + (size_t)io * N + n, fi);
+            put_st<S, STREAM>(f + (size_t)i * N + n, fo);
         } else {
-            S::st(f + (size_t)i * N + nb.of(n, i), fi);
-            S::st(f + (size_t)io * N + nb.of(n, io), fo);
+            put_st<S, STREAM>(f + (size_t)i * N + nb.of(n, i), fi);
+            put_st<S, STREAM>(f + (size_t)io * N + nb.of(n, io), fo);
         }
         if (do_mass) { out.mass += fi; out.mass += fo; }
     }
@@ -506,9 +514,9 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
         if (!boundary) {   // every neighbour fluid: the pair form, same bits
             if (L.force_free)
-                plain_pairs_fp64<S, PAR, false>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+                plain_pairs_fp64<S, PAR, false, !GENERAL>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
             else
-                plain_pairs_fp64<S, PAR, true>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+                plain_pairs_fp64<S, PAR, true, !GENERAL>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
             return;
         }
         // TRT + Guo forcing (lbm.cpp:162-172), in the pair form
@@ -567,9 +575,9 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         shifted_terms<S>(L, rho, u, v, wz, k15, uF, srho);
         if (!boundary) {
             if (L.force_free)   // uniform: the Guo source terms are exactly zero
-                plain_pairs<S, PAR, false>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, false, !GENERAL>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
             else
-                plain_pairs<S, PAR, true>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, true, !GENERAL>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
         } else {
             AR post[Q];
             post[0] = rest_post<S, true>(L, (AR)d[0], dr, srho, k15, uF);
@@ -794,24 +802,24 @@ __device__ __forceinline__ void pair_collide_store(const Lattice& L, const Strea
     auto put = [&](int i, float a0, float a1) {
         if (PAR == 0) {                                        // A[opp(i)][n]
             T* p = f + (size_t)OPP(i) * N + pr.n0;
-            if (act0 && act1) S::st2(p, a0, a1);
-            else { if (act0) S::st(p, a0); if (act1) S::st(p + 1, a1); }
+            if (act0 && act1) S::st2_cs(p, a0, a1);
+            else { if (act0) S::st_cs(p, a0); if (act1) S::st_cs(p + 1, a1); }
             return;
         }
         T* rowp = f + (size_t)i * N + (size_t)((int)pr.row + pr.ryz(i));   // A[i][n + c_i]
         if (CX(i) == 0) {
-            if (act0 && act1) S::st2(rowp + x0, a0, a1);
-            else { if (act0) S::st(rowp + x0, a0); if (act1) S::st(rowp + x0 + 1, a1); }
+            if (act0 && act1) S::st2_cs(rowp + x0, a0, a1);
+            else { if (act0) S::st_cs(rowp + x0, a0); if (act1) S::st_cs(rowp + x0 + 1, a1); }
         } else if (CX(i) > 0) {                                // targets x0 + 1, x0 + 2
             const float pv = __shfl_up_sync(0xffffffffu, a1, 1);
-            if (pr.prev_act1 && act0) S::st2(rowp + x0, pv, a0);
-            else { if (pr.prev_act1) S::st(rowp + x0, pv); if (act0) S::st(rowp + x0 + 1, a0); }
-            if (!pr.has_next && act1) S::st(rowp + pr.xp, a1);
+            if (pr.prev_act1 && act0) S::st2_cs(rowp + x0, pv, a0);
+            else { if (pr.prev_act1) S::st_cs(rowp + x0, pv); if (act0) S::st_cs(rowp + x0 + 1, a0); }
+            if (!pr.has_next && act1) S::st_cs(rowp + pr.xp, a1);
         } else {                                               // targets x0 - 1, x0
             const float nv = __shfl_down_sync(0xffffffffu, a0, 1);
-            if (act1 && pr.next_act0) S::st2(rowp + x0, a1, nv);
-            else { if (act1) S::st(rowp + x0, a1); if (pr.next_act0) S::st(rowp + x0 + 1, nv); }
-            if (!pr.has_prev && act0) S::st(rowp + pr.xm, a0);
+            if (act1 && pr.next_act0) S::st2_cs(rowp + x0, a1, nv);
+            else { if (act1) S::st_cs(rowp + x0, a1); if (pr.next_act0) S::st_cs(rowp + x0 + 1, nv); }
+            if (!pr.has_prev && act0) S::st_cs(rowp + pr.xm, a0);
         }
     };
     pair_collide<S, PAR, FORCE>(L, a, d0, d1, put);

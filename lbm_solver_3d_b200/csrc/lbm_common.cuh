@@ -71,6 +71,8 @@ struct StoreF64 {
     static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static double ld(const T* p) { return *p; }
     __device__ static void st(T* p, double v) { *p = v; }
+    // streaming store (evict first): the bulk's stores, read again only next step
+    __device__ static void st_cs(T* p, double v) { __stcs(p, v); }
     __device__ static double rt(double v) { return v; }  // value as it will be stored
 };
 struct StoreF32 {
@@ -81,9 +83,11 @@ struct StoreF32 {
     static constexpr float SC = 1.0f, INV = 1.0f;
     __device__ static float ld(const T* p) { return *p; }
     __device__ static void st(T* p, float v) { *p = v; }
+    __device__ static void st_cs(T* p, float v) { __stcs(p, v); }
     __device__ static float rt(float v) { return v; }
     __device__ static float2 ld2(const T* p) { return *reinterpret_cast<const float2*>(p); }
     __device__ static void st2(T* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+    __device__ static void st2_cs(T* p, float a, float b) { __stcs(reinterpret_cast<float2*>(p), make_float2(a, b)); }
 };
 constexpr float FP16_SCALE = 4096.0f, FP16_INV_SCALE = 1.0f / 4096.0f;
 struct StoreF16 {
@@ -94,10 +98,17 @@ struct StoreF16 {
     static constexpr float SC = FP16_SCALE, INV = FP16_INV_SCALE;
     __device__ static float ld(const T* p) { return __half2float(*p); }
     __device__ static void st(T* p, float v) { *p = __float2half_rn(v); }
+    __device__ static void st_cs(T* p, float v) {
+        __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(v)));
+    }
     __device__ static float rt(float v) { return __half2float(__float2half_rn(v)); }
     __device__ static float2 ld2(const T* p) { return __half22float2(*reinterpret_cast<const __half2*>(p)); }
     __device__ static void st2(T* p, float a, float b) {
         *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+    }
+    __device__ static void st2_cs(T* p, float a, float b) {
+        const __half2 h = __floats2half2_rn(a, b);
+        __stcs(reinterpret_cast<unsigned int*>(p), *reinterpret_cast<const unsigned int*>(&h));
     }
 };
 
