@@ -542,7 +542,7 @@ def bench_ensemble(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", default=None, choices=list(BYTES))
     ap.add_argument("--workload", default="bulk_0")

@@ -21,6 +21,13 @@
 
 namespace lbmgpu {
 
+// Streaming stores in the ensemble's bulk kernels: FP16 storage only. In FP32
+// storage they made the chunk kernel slower (5.18 -> 5.61 ms for 256 members),
+// its partly written lines leaving L2 before the neighbouring warps fill them.
+template <class S>
+constexpr bool ens_stream() { return sizeof(typename S::T) == 2; }
+
+
 
 // Rows of at most BATCH_MAX_NX nodes: the partial sums of a row are formed
 // exactly as k_bulk forms them for a row held by one block of ceil32(nx)
@@ -86,7 +93,7 @@ __global__ void __launch_bounds__(256) k_bulk_batch(const Lattice* __restrict__ 
                 if (x < L.nx) {
                     const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
                     const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[slot], x, y, z);
-                    if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, wr, MACRO, sums);
+                    if (active) update_node<S, PAR, false, MACRO, ens_stream<S>()>(L, a, n, x, y, z, 0, wr, MACRO, sums);
                 }
                 if (sums_on) {
                     chunk_reduce(sums);
@@ -155,7 +162,7 @@ __global__ void __launch_bounds__(ROWCTA_THREADS, batch_min_blocks<S>()) k_bulk_
         if (x < L.nx) {
             const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
             const bool active = (sA.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ, x, y, z);
-            if (active) update_node<S, PAR, false, MACRO>(L, sA, n, x, y, z, 0, WR ? wall_row(L, y, z) : (uint8_t)0, MACRO, sums);
+            if (active) update_node<S, PAR, false, MACRO, ens_stream<S>()>(L, sA, n, x, y, z, 0, WR ? wall_row(L, y, z) : (uint8_t)0, MACRO, sums);
         }
         if (sums_on) {
             chunk_reduce(sums);
@@ -224,7 +231,7 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, batch_min_blocks<S>()) k_bul
     if (x < L.nx) {
         const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)cr.y + (unsigned)L.ny * (unsigned)cr.z);
         const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, cr.y, cr.z);
-        if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, cr.y, cr.z, 0, 0, MACRO, sums);
+        if (active) update_node<S, PAR, false, MACRO, ens_stream<S>()>(L, a, n, x, cr.y, cr.z, 0, 0, MACRO, sums);
     }
     if (st.do_mass || MACRO) {
         chunk_reduce(sums);
@@ -295,7 +302,7 @@ __global__ void __launch_bounds__(32 * CHUNK_WARPS, batch_min_blocks<S>()) k_bul
         if (on) {
             const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)cr.z);
             const bool active = (a.flag[n] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, sZ[w], x, y, cr.z);
-            if (active) update_node<S, PAR, false, MACRO>(L, a, n, x, y, cr.z, 0, 0, MACRO, sums);
+            if (active) update_node<S, PAR, false, MACRO, ens_stream<S>()>(L, a, n, x, y, cr.z, 0, 0, MACRO, sums);
         }
         if (!FLAT && (st.do_mass || MACRO)) {
             chunk_reduce(sums);
@@ -613,7 +620,7 @@ __global__ void __launch_bounds__(STAGED_THREADS) k_bulk_staged(const Lattice* _
                 const unsigned n = (unsigned)x + (unsigned)L.nx * ((unsigned)y + (unsigned)L.ny * (unsigned)z);
                 const bool active = (sf[x] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, recZ[slot], x, y, z);
                 if (active)
-                    update_node<S, PAR, false, MACRO>(L, a, n, x, y, z, 0, 0, MACRO, sums,
+                    update_node<S, PAR, false, MACRO, ens_stream<S>()>(L, a, n, x, y, z, 0, 0, MACRO, sums,
                                                       StagedSrc<T>{sb, sOff[q], cap, x, L.nx});
             }
             if (sums_on) {
@@ -830,7 +837,7 @@ __global__ void __launch_bounds__(RUNS_THREADS, 2) k_bulk_runs(const Lattice* __
                 const bool active = (sf[j] & (uint8_t)~NEAR_WALL) == 0 && !in_zone(L, recZ[slot], x, y, run.z);
                 if (active) {
                     NodeSums sums;
-                    update_node<S, PAR, false, false>(L, a, n0 + (unsigned)j, x, y, run.z, 0, 0, false, sums,
+                    update_node<S, PAR, false, false, ens_stream<S>()>(L, a, n0 + (unsigned)j, x, y, run.z, 0, 0, false, sums,
                                                       RunSrc<T>{sb, sOff[q], CAP, x, L.nx, row});
                 }
             }

@@ -470,7 +470,8 @@ __device__ __forceinline__ void collide_pairs_fp64(const Lattice& L, const doubl
     }
 }
 
-template <class S, int PAR, bool GENERAL, bool MACRO, class Src = GlobalSrc>
+// STREAM: the plain nodes' stores are streaming stores (plain_pairs).
+template <class S, int PAR, bool GENERAL, bool MACRO, bool STREAM = !GENERAL, class Src = GlobalSrc>
 __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& a, unsigned n, int x, int y, int z,
                                             uint8_t fl, uint8_t wallrow, bool store_rho, NodeSums& out,
                                             const Src& src = Src(), LinkStash<S>* link_stash = nullptr) {
@@ -514,9 +515,9 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         const double usq = u * u + v * v + wz * wz, uF = u * Fx + v * Fy + wz * Fz;
         if (!boundary) {   // every neighbour fluid: the pair form, same bits
             if (L.force_free)
-                plain_pairs_fp64<S, PAR, false, !GENERAL>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+                plain_pairs_fp64<S, PAR, false, STREAM>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
             else
-                plain_pairs_fp64<S, PAR, true, !GENERAL>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
+                plain_pairs_fp64<S, PAR, true, STREAM>(L, f, N, n, nb, fv, r, u, v, wz, usq, uF, do_mass, out);
             return;
         }
         // TRT + Guo forcing (lbm.cpp:162-172), in the pair form
@@ -575,9 +576,9 @@ __device__ __forceinline__ void update_node(const Lattice& L, const StreamArgs& 
         shifted_terms<S>(L, rho, u, v, wz, k15, uF, srho);
         if (!boundary) {
             if (L.force_free)   // uniform: the Guo source terms are exactly zero
-                plain_pairs<S, PAR, false, !GENERAL>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, false, STREAM>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
             else
-                plain_pairs<S, PAR, true, !GENERAL>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
+                plain_pairs<S, PAR, true, STREAM>(L, f, N, n, nb, d, dr, srho, u, v, wz, uF, k15, do_mass, out);
         } else {
             AR post[Q];
             post[0] = rest_post<S, true>(L, (AR)d[0], dr, srho, k15, uF);
