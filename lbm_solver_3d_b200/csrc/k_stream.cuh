@@ -276,6 +276,58 @@ __device__ __forceinline__ void shifted_terms(const Lattice& L, A rho, A u, A v,
 // weight class of direction i: 0 rest, 1 axes, 2 diagonals
 __host__ __device__ constexpr int wclass(int i) { return i == 0 ? 0 : (i <= 6 ? 1 : 2); }
 
+// Two nodes' FP32 numbers side by side (element 0: the first node, element 1:
+// the second) and the sm_100 paired FP32 FMA on them (PTX fma.rn.f32x2: each
+// element rounded once, as __fmaf_rn rounds it).
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    unsigned long long r, pa, pb, pc;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(pc) : "f"(c.x), "f"(c.y));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pa), "l"(pb), "l"(pc));
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+
+// Paired adds, subtracts and multiplies, each written as that FMA with a
+// constant the compiler cannot see (Lattice::one = 1, Lattice::mzero = -0):
+//   a + b = fma(a, 1, b),  a - b = fma(b, -1, a),  a * b = fma(a, b, -0).
+// x * 1 and x * -1 are exact and p + (-0) = p for every p, signed zeros
+// included, so each is the IEEE result of the scalar __fadd_rn / __fsub_rn /
+// __fmul_rn bit for bit; and as FMAs with unknown operands they are neither
+// fused with their neighbours nor reordered. (Written as the plain paired add
+// and multiply instructions instead, the two-node results were measured to
+// differ from the one-node ones in the last place.)
+struct Paired {
+    float2 one, mone, mz;
+    __device__ __forceinline__ explicit Paired(const Lattice& L)
+        : one(bc2(L.one)), mone(bc2(-L.one)), mz(bc2(L.mzero)) {}
+    __device__ __forceinline__ float2 add(float2 a, float2 b) const { return fma2(a, one, b); }
+    __device__ __forceinline__ float2 sub(float2 a, float2 b) const { return fma2(b, mone, a); }
+    __device__ __forceinline__ float2 mul(float2 a, float2 b) const { return fma2(a, b, mz); }
+};
+
+// c_i . u in FP32 for a moving direction (one or two nonzero components, each
+// -1 or 1): the terms in x, y, z order and one explicit rounded sum, formed the
+// same way by the one-node (V = float) and the two-node (V = float2) code.
+__device__ __forceinline__ float cdot_neg(float a) { return -a; }
+__device__ __forceinline__ float2 cdot_neg(float2 a) { return neg2(a); }
+struct ScalarAdd {
+    __device__ __forceinline__ float add(float a, float b) const { return __fadd_rn(a, b); }
+};
+template <class V, class Ops>
+__device__ __forceinline__ V cdot_f(int i, V u, V v, V wz, const Ops& op) {
+    V t[3];
+    int k = 0;
+    if (CX(i) != 0) t[k++] = CX(i) > 0 ? u : cdot_neg(u);
+    if (CY(i) != 0) t[k++] = CY(i) > 0 ? v : cdot_neg(v);
+    if (CZ(i) != 0) t[k++] = CZ(i) > 0 ? wz : cdot_neg(wz);
+    return k == 1 ? t[0] : op.add(t[0], t[1]);
+}
+
 // TRT + Guo post-collision values in storage units (lbm.cpp:162-172, deviation
 // form), in the form's arithmetic A: the rest population, and one opposite pair
 // (i, i+1). srho = S::SC * rho, k15 = 1.5 |u|^2, uF = u . F. FORCE = false
@@ -303,9 +355,9 @@ template <class S, bool FORCE, class A = typename S::A>
 __device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, A u, A v, A wz, A dr, A srho, A k15,
                                           A uF, A& oi, A& oo) {
     using C = Coll<A>;
-    const A cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
     const A w = C::w(i);
     if constexpr (sizeof(A) == 4) {
+        const float cu = cdot_f<float>(i, u, v, wz, ScalarAdd());
         // every operation spelled out, so that no kernel contracts it differently
         const int c = wclass(i);
         const float eP = __fmul_rn(C::w(i), __fmaf_rn(srho, __fmaf_rn(__fmul_rn(4.5f, cu), cu, -k15), dr));
@@ -320,6 +372,7 @@ __device__ __forceinline__ void pair_post(const Lattice& L, int i, A di, A dio, 
         oi = __fadd_rn(__fadd_rn(di, a), b);
         oo = __fsub_rn(__fadd_rn(dio, a), b);
     } else {
+        const A cu = CX(i) * u + CY(i) * v + CZ(i) * wz;
         const A eP = w * (dr + srho * (A(4.5) * cu * cu - k15));   // feq+ - w, storage units
         const A eM = A(3) * w * srho * cu;                          // feq-
         const A fP = A(0.5) * (di + dio), fM = A(0.5) * (di - dio);
@@ -766,6 +819,50 @@ __device__ __forceinline__ void pair_collide(const Lattice& L, const StreamArgs&
         }
     }
     using AR = typename S::A;
+    if constexpr (sizeof(AR) == 4) {
+        // FP32 arithmetic: the moments and per-node terms node by node, then
+        // the collision of both nodes at once in paired FMAs (Paired), the
+        // operations of rest_post and pair_post<float> in their order, so
+        // each node's values are those of the one-node kernels bit for bit.
+        float dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
+        shifted_moments<S>(L, d0, dr0, rho0, u0, v0, w0);
+        shifted_moments<S>(L, d1, dr1, rho1, u1, v1, w1);
+        float k0, k1, uF0, uF1, sr0, sr1;
+        shifted_terms<S>(L, rho0, u0, v0, w0, k0, uF0, sr0);
+        shifted_terms<S>(L, rho1, u1, v1, w1, k1, uF1, sr1);
+        const Paired op(L);
+        const float2 dr = make_float2(dr0, dr1), u = make_float2(u0, u1), v = make_float2(v0, v1),
+                     wz = make_float2(w0, w1), k15 = make_float2(k0, k1), uF = make_float2(uF0, uF1),
+                     srho = make_float2(sr0, sr1);
+        {   // rest population
+            const float2 d = make_float2(d0[0], d1[0]);
+            const float2 eP = op.mul(bc2(WF(0)), fma2(neg2(srho), k15, dr));
+            float2 o = fma2(bc2(-L.omPf), op.sub(d, eP), d);
+            if (FORCE) o = fma2(bc2(-3.0f * S::SC * L.gPw[0]), uF, o);
+            put(0, o.x, o.y);
+        }
+#pragma unroll
+        for (int i = 1; i < Q; i += 2) {
+            const float2 di = make_float2(d0[i], d1[i]), dio = make_float2(d0[i + 1], d1[i + 1]);
+            const float2 cu = cdot_f<float2>(i, u, v, wz, op);
+            const float2 eP = op.mul(bc2(WF(i)), fma2(srho, fma2(op.mul(bc2(4.5f), cu), cu, neg2(k15)), dr));
+            const float2 eM = op.mul(op.mul(bc2(3.0f * WF(i)), srho), cu);
+            const float2 fP = op.mul(bc2(0.5f), op.add(di, dio));
+            const float2 fM = op.mul(bc2(0.5f), op.sub(di, dio));
+            float2 ta = op.mul(bc2(-L.omPf), op.sub(fP, eP));
+            float2 tb = op.mul(bc2(-L.omMf), op.sub(fM, eM));
+            if (FORCE) {
+                ta = fma2(bc2(S::SC * L.gPw[wclass(i)]),
+                          fma2(op.mul(bc2(9.0f), cu), bc2(L.cF[i]), op.mul(bc2(-3.0f), uF)), ta);
+                tb = op.add(tb, bc2(S::SC * L.cm[i]));
+            }
+            const float2 oi = op.add(op.add(di, ta), tb);
+            const float2 oo = op.sub(op.add(dio, ta), tb);
+            put(i, oi.x, oi.y);
+            put(i + 1, oo.x, oo.y);
+        }
+        return;
+    }
     AR dr0, rho0, u0, v0, w0, dr1, rho1, u1, v1, w1;
     shifted_moments<S>(L, d0, dr0, rho0, u0, v0, w0);
     shifted_moments<S>(L, d1, dr1, rho1, u1, v1, w1);

@@ -127,6 +127,10 @@ struct Lattice {
     float gPw[3];
     float cF[Q], cm[Q];
     int force_free;        // F = 0: the Guo source terms vanish (FP32 arithmetic skips them)
+    // 1 and -0, held in the kernel argument so that the compiler cannot see
+    // their values: the two-node FP32 arithmetic forms every operation as an
+    // FMA with one of them (k_stream.cuh, Paired)
+    float one, mzero;
 };
 
 // ---- the zone around the sphere ----------------------------------------------

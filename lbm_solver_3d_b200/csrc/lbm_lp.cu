@@ -1,5 +1,6 @@
-// FP32-shifted and FP16-storage forms (deviations f_i - w_i stored, FP32
-// arithmetic, FP64 boundary-link sums and rigid body).
+// FP32-shifted and FP16-storage forms (deviations f_i - w_i stored; FP64
+// arithmetic for FP32 storage and FP32 arithmetic for FP16 storage; FP64
+// boundary-link sums and rigid body).
 #include "lbm_launch_impl.cuh"
 
 namespace lbmgpu {

@@ -711,6 +711,8 @@ int create_impl(const lbmgpu_params* p, const MemberOpts* mo, lbmgpu_handle** ou
     for (int c = 0; c < 3; ++c) L.gPw[c] = (float)(L.gP * (c == 0 ? WD(0) : (c == 1 ? WD(1) : WD(7))));
     for (int d = 0; d < 3; ++d) { L.Ff[d] = (float)L.F[d]; L.uFh[d] = 0.0f; }
     L.force_free = L.F[0] == 0.0 && L.F[1] == 0.0 && L.F[2] == 0.0;
+    L.one = 1.0f;
+    L.mzero = -0.0f;
     for (int i = 0; i < Q; ++i) {
         const double cF = CX(i) * L.F[0] + CY(i) * L.F[1] + CZ(i) * L.F[2];
         L.cF[i] = (float)cF;

@@ -76,8 +76,10 @@ class Ensemble:
     STAGED2, STAGED3 = -2, -3
 
     def set_tiling(self, tile: int, ctas_per_sm: int) -> None:
-        """tile 32/64/128: threads per row of the row kernel; -2/-3: the staged
-        kernel with 2/3 shared-memory stages."""
+        """tile 32/64/128: threads per row of the row kernel; 1: one CTA per
+        row; 2 / 3: 32-node chunks (3: persistent warps); 4: staged row runs;
+        -3 / -4: the staged kernel with 3 / 4 shared-memory stages
+        (include/lbmgpu.h, LBMGPU_TILE_*)."""
         check_batch(self.lib.lbmgpu_batch_set_tiling(self.b, int(tile), int(ctas_per_sm)), self.b)
         self.tiling = (tile, ctas_per_sm)
 

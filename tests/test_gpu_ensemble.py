@@ -105,7 +105,7 @@ def test_ensemble_autotune_restores_state(api):
     with Ensemble(ps) as ens:
         ens.run(30)
         tuned = ens.autotune(reps=2)
-        assert tuned["tile"] in (1, 2, 3, 32, 64, 128, -3, -4) and 1 <= tuned["ctas_per_sm"] <= 16
+        assert tuned["tile"] in (1, 2, 3, 4, 32, 64, 128, -3, -4) and 1 <= tuned["ctas_per_sm"] <= 16
         assert tuned["ms"] > 0
         ens.run(40)
         for i in range(len(ps)):
